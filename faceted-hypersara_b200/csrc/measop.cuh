@@ -1,0 +1,106 @@
+// Measurement operator Phi = G A on the device (see measop.cu).
+#pragma once
+
+#include "common.cuh"
+#include "minmax.h"
+
+namespace fhs {
+
+// Read-only view of the operator passed to kernels by value.
+struct OpView {
+  int Ny, Nx, Ky, Kx, Jy, Jx;
+  int nT0, nT1;      // tiles per axis (kTileCells cells each, last may be partial)
+  int nsb0, nsb1;    // sub-bins per axis (kBinCells cells each)
+  int nkeys;         // nT0*nT1*kSubPerTile^2 sort keys per channel
+  const float2* tab_y;  // [Jy][kTableSamples+1]
+  const float2* tab_x;  // [Jx][kTableSamples+1]
+  const float* sy;      // [Ny] scaling factors
+  const float* sx;      // [Nx]
+  const float4* geom;   // per sorted visibility: (fy, fx, kpack bits, weight)
+  const int32_t* sb_off;  // [L][nkeys+1] visibility offsets per sub-bin (channel-relative)
+  const int64_t* ch_voff; // [L] first visibility of each channel
+  const int32_t* ch_M;    // [L]
+};
+
+struct ChannelHost {
+  std::vector<float4> geom;        // sorted order
+  std::vector<int32_t> perm;       // sorted position -> original index
+  std::vector<int32_t> sb_off;     // nkeys+1
+  std::vector<int64_t> block_sizes;
+  int64_t M = 0;
+  bool set = false;
+};
+
+struct MeasOp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int Ny = 0, Nx = 0, Ky = 0, Kx = 0, Jy = 7, Jx = 7, L = 0;
+  int nT0 = 0, nT1 = 0, nsb0 = 0, nsb1 = 0, nkeys = 0;
+  MinMaxAxis ay, ax;
+  std::vector<ChannelHost> ch;
+  bool committed = false;
+
+  // host copies of the channel layout
+  std::vector<int64_t> h_voff;     // [L]
+  std::vector<int32_t> h_M;        // [L]
+  std::vector<int32_t> h_blkoff;   // [L] first block of each channel (global block index)
+  std::vector<int32_t> h_nblk;     // [L]
+  int64_t Mtot = 0;
+  int nblk_tot = 0;
+  int64_t maxM = 0;
+
+  DevBuf<float2> tab_y, tab_x;
+  DevBuf<float> sy, sx;
+  DevBuf<float4> geom;
+  DevBuf<int32_t> perm;
+  DevBuf<int32_t> sb_off;
+  DevBuf<int64_t> ch_voff;
+  DevBuf<int32_t> ch_M, ch_blkoff, ch_nblk;
+
+  // grids: pad (FFT input, zero outside the image), A (FFT output / IFFT
+  // output), B (gridding output, IFFT input).  [L][Kx][Ky] each.
+  DevBuf<float2> pad, gridA, gridB;
+  cufftHandle plan_all = 0, plan_one = 0;
+
+  // scratch for API-level calls
+  DevBuf<float2> vis_a, vis_b;
+  DevBuf<double> stage;     // host-format staging (double)
+  DevBuf<float> img_a;      // [L][N] image scratch
+  DevBuf<double> partials;  // [L][ntiles][kMaxBlocksPerChannel][2]
+  DevBuf<double> blk_stats; // [nblk_tot][2]: ||z||^2, ||res||^2
+  DevBuf<float> blk_scale;  // [L][kMaxBlocksPerChannel]
+  DevBuf<double> blk_eps;   // [L][kMaxBlocksPerChannel]
+
+  int64_t No() const { return (int64_t)Ky * Kx; }
+  int64_t Npix() const { return (int64_t)Ny * Nx; }
+  int ntiles() const { return nT0 * nT1; }
+  OpView view() const;
+  ~MeasOp();
+};
+
+MeasOp* measop_create(int device, int Ny, int Nx, int oy, int ox, int Jy, int Jx, int L);
+void measop_set_channel(MeasOp* op, int channel, int64_t n, const double* om_y, const double* om_x,
+                        const double* w, int n_blocks, const int64_t* block_sizes);
+void measop_commit(MeasOp* op);
+
+// ---- device building blocks used by the API and the solver -------------
+// pad[l] <- s .* x[l] at (n - N/2) mod K (planes [p0, p0+np)); x: [np][N] f32
+void launch_pad(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s);
+// FFT of pad planes -> gridA (forward), or gridB -> gridA (inverse)
+void fft_forward(const MeasOp* op, int p0, int np, cudaStream_t s);
+void fft_inverse(const MeasOp* op, int p0, int np, cudaStream_t s);
+// GFx for channels [c0, c0+nc) from gridA into out (sorted visibility order)
+void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s);
+// gridB <- G^H v (v sorted, channels [c0, c0+nc)); non-empty tiles only
+void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
+// out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1
+void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s);
+// fused dual update, pass 1: GFx, z -> v2, GFx -> gold, block partials
+void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
+                        cudaStream_t s);
+// block reduction: scale = 1 - min(eps/||z||, 1); stats for the report
+void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s);
+// fused dual update, pass 2: v2 <- z*scale, gridB <- G^H v2
+void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s);
+
+}  // namespace fhs

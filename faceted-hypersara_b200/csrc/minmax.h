@@ -1,0 +1,19 @@
+// Host-side FP64 min-max NUFFT interpolator tables (see minmax.cpp).
+#pragma once
+
+#include <vector>
+
+namespace fhs {
+
+struct MinMaxAxis {
+  int N = 0, K = 0, J = 0, n_samples = 0;
+  std::vector<double> cos_coefs;  // scaling cosine series a_0..a_L
+  std::vector<double> scale;      // s_n, n = 0..N-1
+  std::vector<double> table_re;   // h_j(dk) real part, [J][n_samples+1]
+  std::vector<double> table_im;   // imaginary part
+};
+
+// Tables for one axis: N image pixels, K grid cells, J taps.
+MinMaxAxis build_minmax_axis(int N, int K, int J, int n_samples, int n_cos = 6);
+
+}  // namespace fhs

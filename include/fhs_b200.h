@@ -1,0 +1,213 @@
+/*
+ * fhs_b200.h -- C ABI of the B200 (sm_100a) Faceted HyperSARA library.
+ *
+ * Drop-in boundary for the reference's MATLAB entry points
+ * (basp-group/Faceted-HyperSARA).  A MEX gateway (or ctypes, or a C program)
+ * binds these functions; every buffer is a plain host pointer in MATLAB's
+ * memory order:
+ *   - image cubes  x[Ny, Nx, L]  double, column-major (y fastest);
+ *   - grids        Fx[No]        complex double, interleaved (re, im),
+ *                  column-major over (Ky = oy*Ny, Kx = ox*Nx);
+ *   - visibilities y[M]          complex double, interleaved, channel after
+ *                  channel, blocks of a channel concatenated in block order.
+ * The library copies host buffers in and out and owns all device memory of a
+ * handle.  No exception, exit() or abort() crosses this boundary: every call
+ * returns an fhs_status and fhs_last_error() gives the message (thread-local).
+ * A handle binds one CUDA device and one stream; handles are independent and
+ * may be used from different host threads, one thread per handle at a time.
+ */
+#ifndef FHS_B200_H
+#define FHS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FHS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FHS_API __attribute__((visibility("default")))
+#else
+#define FHS_API
+#endif
+
+typedef enum fhs_status {
+  FHS_OK = 0,
+  FHS_ERR_INVALID_ARG = 1,   /* bad size, index, pointer or parameter */
+  FHS_ERR_CUDA = 2,          /* CUDA runtime / cuFFT failure */
+  FHS_ERR_OUT_OF_MEMORY = 3, /* device allocation failed */
+  FHS_ERR_STATE = 4,         /* call made in the wrong order */
+  FHS_ERR_NUMERIC = 5,       /* non-finite value detected */
+  FHS_ERR_UNSUPPORTED = 6,   /* configuration outside the supported limits */
+  FHS_ERR_NO_DEVICE = 7      /* no CUDA device / driver */
+} fhs_status;
+
+/* ABI version of the loaded library (FHS_ABI_VERSION it was built with). */
+FHS_API int fhs_abi_version(void);
+/* Message of the last failed call on this host thread ("" if none). */
+FHS_API const char* fhs_last_error(void);
+/* Number of kernels this library launched since load (all handles). */
+FHS_API unsigned long long fhs_kernel_launch_count(void);
+
+/* ======================================================================
+ * Measurement operator  Phi_l = G_l A  (replaces op_p_nufft of the
+ * RI-measurement-operator submodule, built at
+ * lib/operators/util_gen_measurement_operator_synth.m:86 and applied by
+ * lib/operators/HS_forward_operator_G.m:36-52 / HS_adjoint_operator_G.m:42-57).
+ * Min-max interpolation (Fessler & Sutton 2003), J taps per axis, 2-D
+ * separable, scaling factors from a Kaiser-Bessel cosine series.
+ * Limits: Ky = oy*Ny and Kx = ox*Nx multiples of 8 and <= 16384, Ny and Nx
+ * even, 2 <= J <= 8, at most 16 blocks per channel.  The mask W of the
+ * reference is the full grid (every G column is addressable).
+ * ====================================================================== */
+typedef struct fhs_measop fhs_measop;
+
+FHS_API fhs_status fhs_measop_create(int device, int Ny, int Nx, int oy, int ox, int Jy, int Jx,
+                             int n_channels, fhs_measop** out);
+FHS_API fhs_status fhs_measop_destroy(fhs_measop* op);
+/* Visibilities of one channel: frequencies (radians, om_y = v, om_x = u as
+ * in op_p_nufft([{v} {u}], ...)), optional per-visibility weights (the noise
+ * whitening folded into G's rows; NULL = 1), block sizes summing to n_vis. */
+FHS_API fhs_status fhs_measop_set_channel(fhs_measop* op, int channel, int64_t n_vis, const double* om_y,
+                                  const double* om_x, const double* weights, int n_blocks,
+                                  const int64_t* block_sizes);
+/* Finalise (device upload, visibility binning, FFT plans).  Required once
+ * after all channels are set and before any apply call. */
+FHS_API fhs_status fhs_measop_commit(fhs_measop* op);
+FHS_API int64_t fhs_measop_n_vis(const fhs_measop* op, int channel);
+FHS_API int64_t fhs_measop_grid_size(const fhs_measop* op); /* No = Ky*Kx */
+
+/* A (op_nufft's scaled zero-padded FFT; shape contract of
+ * src/apply_scaled_fourier_transform.m:21-24): x[Ny,Nx] -> Fx[No] complex. */
+FHS_API fhs_status fhs_scaled_fft(fhs_measop* op, const double* x, double* Fx);
+/* At (exact adjoint of A): Fx[No] complex -> x[Ny,Nx] complex. */
+FHS_API fhs_status fhs_scaled_fft_adjoint(fhs_measop* op, const double* Fx, double* x_complex);
+/* src/apply_direct_operator.m:1  y = G Fx  (Lambda = 1, no DR). */
+FHS_API fhs_status fhs_apply_direct_operator(fhs_measop* op, int channel, const double* Fx, double* y);
+/* src/apply_adjoint_operator.m:1  Fx = G' y  (Lambda = 1, no DR). */
+FHS_API fhs_status fhs_apply_adjoint_operator(fhs_measop* op, int channel, const double* y, double* Fx);
+/* lib/operators/HS_forward_operator_G.m:36-52: x[Ny,Nx,L] -> y (all channels). */
+FHS_API fhs_status fhs_forward_operator(fhs_measop* op, const double* x, double* y);
+/* lib/operators/HS_adjoint_operator_G.m:42-57 followed by real(): y -> x[Ny,Nx,L]. */
+FHS_API fhs_status fhs_adjoint_operator(fhs_measop* op, const double* y, double* x);
+/* lib/utils/util_operator_norm.m:43-61: per-channel ||G_l A||^2 by power
+ * iteration (op_norm of the submodule), FP32 operators, FP64 norms. */
+FHS_API fhs_status fhs_operator_norm(fhs_measop* op, int max_iter, double tol, double* squared_norms);
+
+/* src/update_dual_data_fidelity.m:116-147 (pU = 1, no DR) on host buffers.
+ * v2, y: all channels' visibilities; x[Ny,Nx,L]; Fx_old[No,L] complex
+ * (updated to A(x)); epsilon: one per block (channel-major); sigma22[L].
+ * Outputs: v2 (updated), Ftx[Ny,Nx,L], norm_res (one per block),
+ * global_norm_res and norm_epsilon (sums of squares, as the reference). */
+FHS_API fhs_status fhs_update_dual_data_fidelity(fhs_measop* op, double* v2, const double* y,
+                                         const double* x, double* Fx_old, const double* epsilon,
+                                         const double* sigma22, double* Ftx, double* norm_res,
+                                         double* global_norm_res, double* norm_epsilon);
+
+/* ======================================================================
+ * Priors (standalone, device selected per call)
+ * ====================================================================== */
+/* src/proj_l2ball.m:20-22  p = y + (x-y) min(eps/||x-y||, 1); complex n-vectors, FP64. */
+FHS_API fhs_status fhs_proj_l2ball(int device, int64_t n, const double* x, double eps, const double* y,
+                           double* p);
+/* src/nuclear_norm.m:25-26  sum of singular values of x reshaped [N, L]. */
+FHS_API fhs_status fhs_nuclear_norm(int device, int64_t n_pixels, int L, const double* x, double* f);
+/* SARA dictionary (op_p_sp_wlt_basis of the SARA-dictionary submodule,
+ * imaging/imaging.m:802): db1..db8 + Dirac, nlevel levels, zero padding,
+ * 1/sqrt(9) normalisation.  Coefficients per channel, wavedec2 layout per
+ * basis, bases concatenated.  n_coefs returns s (per channel). */
+FHS_API int64_t fhs_sara_n_coefs(int Ny, int Nx, int nlevel);
+FHS_API fhs_status fhs_sara_analysis(int device, int Ny, int Nx, int L, int nlevel, const double* x,
+                             double* coefs);
+FHS_API fhs_status fhs_sara_synthesis(int device, int Ny, int Nx, int L, int nlevel, const double* coefs,
+                              double* x);
+/* src/compute_sara_prior.m:35-41  sum_i ||(Psit x)_i||_2 over channels. */
+FHS_API fhs_status fhs_compute_sara_prior(int device, int Ny, int Nx, int L, int nlevel, const double* x,
+                                  double* f);
+
+/* ======================================================================
+ * Solver: the primal-dual iteration of
+ *   facetHyperSARA (src/fhs/facetHyperSARA.m:1-6, loop :701-1138),
+ *   hyperSARA      (src/hs/hyperSARA.m:1-3, loop :565-866),
+ *   sara           (src/sara/sara.m:1-3, loop :521-837),
+ * on the channels of one fhs_measop.  Channels are split into n_groups
+ * equal contiguous spectral sub-cubes solved side by side (independent
+ * problems: each has its own l21 and nuclear-norm priors and parameters).
+ * ====================================================================== */
+typedef enum fhs_algo { FHS_ALGO_SARA = 0, FHS_ALGO_HS = 1, FHS_ALGO_FHS = 2 } fhs_algo;
+typedef enum fhs_window { FHS_WINDOW_NONE = 0, FHS_WINDOW_TRIANGULAR = 1 } fhs_window;
+
+typedef struct fhs_solver_config {
+  int algo;            /* fhs_algo */
+  int nlevel;          /* SARA depth (4) */
+  int n_groups;        /* spectral sub-cubes, channels per group = L / n_groups */
+  int Qy, Qx;          /* spatial facets of the nuclear-norm prior (FHS) */
+  const int* splits_y; /* Qy+1 facet boundaries 0..Ny (NULL: split_range) */
+  const int* splits_x; /* Qx+1 facet boundaries 0..Nx (NULL: split_range) */
+  int overlap_y, overlap_x; /* nuclear-norm facet overlap (pixels) */
+  int window;          /* fhs_window (apodisation of the nuclear facets) */
+} fhs_solver_config;
+
+/* The `param` fields the solvers read (imaging/imaging.m:839-860,
+ * imaging/default_parameters.json).  Arrays: gamma/sig per group,
+ * gamma0/sig_bar per group*Q (group-major), nu2 per channel. */
+typedef struct fhs_solver_params {
+  double nu0, nu1;
+  const double* nu2;
+  const double* gamma;
+  const double* gamma0;
+  const double* reweighting_sig;
+  const double* reweighting_sig_bar;
+  double reweighting_alpha;
+  int reweighting_flag;
+  int reweighting_min_iter, reweighting_max_iter;
+  double reweighting_rel_var;
+  int pdfb_min_iter, pdfb_max_iter;
+  double pdfb_rel_var, pdfb_fidelity_tolerance, pdfb_rel_var_low;
+} fhs_solver_params;
+
+/* Per-iteration record (FP64), summed over all groups. */
+typedef struct fhs_iter_info {
+  double rel_val;         /* sqrt(sum(x-x_prev)^2 / sum x^2) */
+  double residual;        /* sqrt(sum_blocks ||G Fx - y||^2) */
+  double epsilon;         /* sqrt(sum_blocks eps^2) */
+  double nuclear;         /* sum of facet singular values of (v0 + D xhat) before the prox */
+} fhs_iter_info;
+
+typedef struct fhs_run_info {
+  int n_iter;
+  int n_reweights;
+  int converged;
+  double rel_val, residual, epsilon;
+  double seconds;
+} fhs_run_info;
+
+typedef struct fhs_solver fhs_solver;
+
+FHS_API fhs_status fhs_solver_create(fhs_measop* op, const fhs_solver_config* cfg, fhs_solver** out);
+FHS_API fhs_status fhs_solver_destroy(fhs_solver* s);
+/* y: visibilities of all channels (whitened, original order); epsilon: one l2
+ * bound per block, channel-major. */
+FHS_API fhs_status fhs_solver_set_data(fhs_solver* s, const double* y, const double* epsilon);
+FHS_API fhs_status fhs_solver_set_params(fhs_solver* s, const fhs_solver_params* p);
+/* Initial primal cube x[Ny,Nx,L] (NULL = zeros); initialises duals and
+ * weights as fhs_initialize_dual_and_weights.m:88-118 / sara.m:352-362. */
+FHS_API fhs_status fhs_solver_init(fhs_solver* s, const double* xinit);
+/* n PDFB iterations without stopping test or reweighting (graph replays).
+ * info: n records or NULL. */
+FHS_API fhs_status fhs_solver_iterate(fhs_solver* s, int n, fhs_iter_info* info);
+/* Full solve: iterations, PDFB stopping rule (facetHyperSARA.m:877-881) and
+ * reweighting (:952-1137) until convergence or max_iter (<=0: the reference's
+ * (reweighting_max_iter+1)*pdfb_max_iter). */
+FHS_API fhs_status fhs_solver_run(fhs_solver* s, int max_iter, fhs_run_info* info);
+FHS_API fhs_status fhs_solver_get_x(fhs_solver* s, double* x);
+/* Recompute reweighting weights from the current x (fhs_update_weights.m). */
+FHS_API fhs_status fhs_solver_update_weights(fhs_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FHS_B200_H */

@@ -1,0 +1,368 @@
+"""FP64 CPU restatement of the SARA / HyperSARA / Faceted HyperSARA iterations.
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/nufft.py``).
+
+Arrays are channel-first here: an image cube is ``x[L, Ny, Nx]``.  Each
+function cites the reference file it restates.  The preconditioning matrices
+``pU`` are identity (the l2-ball form ``update_dual_data_fidelity.m:83``
+reached by ``solver_proj_elipse_fb`` when ``pU = 1``), and visibility gridding
+(DR) is off.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+from scipy.special import gammaln
+
+from . import wavelets as wv
+from .facets import FacetGeometry
+from .nufft import NufftOperator
+
+MATLAB_EPS = np.finfo(np.float64).eps
+
+
+# ----------------------------------------------------------------- small ops
+def proj_l2ball(x, eps, y):
+    """src/proj_l2ball.m:20-22."""
+    p = x - y
+    nrm = np.linalg.norm(p.ravel())
+    return p * min(eps / nrm, 1.0) + y if nrm > 0 else x.copy()
+
+
+def nuclear_norm(x):
+    """src/nuclear_norm.m:25-26 (x [L, Ny, Nx])."""
+    L = x.shape[0]
+    return float(np.sum(np.linalg.svd(x.reshape(L, -1).T, compute_uv=False)))
+
+
+def compute_sara_prior(x, nlevel=4):
+    """src/compute_sara_prior.m:35-41: sum_i ||(Psit x)_i||_2 over channels."""
+    r = wv.sara_analysis(x, nlevel)
+    return float(np.sum(np.sqrt(np.sum(r * r, axis=0))))
+
+
+def primal_update(x, g):
+    """src/fhs/fhs_update_primal.m:33-38."""
+    xn = np.maximum(x - g, 0.0)
+    xhat = 2.0 * xn - x
+    return xn, xhat, float(np.sum((x - xn) ** 2)), float(np.sum(xn ** 2))
+
+
+# -------------------------------------------------------------- data fidelity
+@dataclass
+class DataTerm:
+    """Per-channel measurement blocks: G[l][b] (csr, whitening folded in), y, eps."""
+    op: NufftOperator
+    G: list
+    y: list
+    eps: list
+
+    @property
+    def L(self):
+        return len(self.G)
+
+
+def forward_operator(x, data: DataTerm):
+    """lib/operators/HS_forward_operator_G.m:36-52 (no DR)."""
+    out = []
+    for l in range(data.L):
+        Fx = data.op.A(x[l])
+        out.append([G @ Fx for G in data.G[l]])
+    return out
+
+
+def adjoint_operator(yb, data: DataTerm):
+    """lib/operators/HS_adjoint_operator_G.m:42-57 (no DR), real part kept."""
+    op = data.op
+    out = np.zeros((data.L, op.Ny, op.Nx))
+    for l in range(data.L):
+        g2 = np.zeros(op.No, dtype=np.complex128)
+        for G, v in zip(data.G[l], yb[l]):
+            g2 += G.conj().T @ v
+        out[l] = np.real(op.At(g2))
+    return out
+
+
+def update_dual_data_fidelity(v2, x, Fx_old, data: DataTerm, sigma22):
+    """src/update_dual_data_fidelity.m:116-147 with pU = 1.
+
+    Returns (v2, Ftx, Fx_old, norm_res, global_norm_res^2, norm_epsilon^2).
+    """
+    op = data.op
+    Ftx = np.zeros_like(x)
+    norm_res = []
+    gres, geps = 0.0, 0.0
+    Fx_new = np.empty_like(Fx_old)
+    v2n = []
+    for l in range(data.L):
+        Fx = op.A(x[l])
+        g2 = np.zeros(op.No, dtype=np.complex128)
+        nr, vl = [], []
+        for b, G in enumerate(data.G[l]):
+            r2 = G @ (2.0 * Fx - Fx_old[l])
+            p = proj_l2ball(v2[l][b] + r2, data.eps[l][b], data.y[l][b])
+            vb = v2[l][b] + r2 - p
+            vl.append(vb)
+            g2 += G.conj().T @ vb
+            res = np.linalg.norm(G @ Fx - data.y[l][b])
+            nr.append(res)
+            gres += res ** 2
+            geps += data.eps[l][b] ** 2
+        v2n.append(vl)
+        norm_res.append(nr)
+        Fx_new[l] = Fx
+        Ftx[l] = sigma22[l] * np.real(op.At(g2))
+    return v2n, Ftx, Fx_new, norm_res, gres, geps
+
+
+def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0):
+    """Squared spectral norm of Phi_l = G_l A per channel by power iteration
+    (lib/utils/util_operator_norm.m:43-61, op_norm of the missing submodule)."""
+    rng = np.random.default_rng(seed)
+    op = data.op
+    out = np.zeros(data.L)
+    for l in range(data.L):
+        x = rng.standard_normal((op.Ny, op.Nx))
+        x /= np.linalg.norm(x)
+        val = 0.0
+        for _ in range(n_iter):
+            Fx = op.A(x)
+            g2 = np.zeros(op.No, dtype=np.complex128)
+            for G in data.G[l]:
+                g2 += G.conj().T @ (G @ Fx)
+            xn = np.real(op.At(g2))
+            new = np.linalg.norm(xn)
+            x = xn / new
+            if abs(new - val) <= tol * new:
+                val = new
+                break
+            val = new
+        out[l] = val
+    return out
+
+
+# ---------------------------------------------------------------- the priors
+def l21_prox_update(v1, xhat, weights1, beta1, nlevel=4):
+    """src/hs/hs_update_dual_sparsity_distributed.m:41-54 (and the faceted
+    src/fhs/fhs_update_dual_sparsity.m:67-93, whose facet coefficients are the
+    global ones).  Returns (v1, Psi v1) (no step size applied)."""
+    r1 = v1 + wv.sara_analysis(xhat, nlevel)
+    l2 = np.sqrt(np.sum(r1 * r1, axis=0))
+    l2_soft = np.maximum(l2 - beta1 * weights1, 0.0) / (l2 + MATLAB_EPS)
+    v1 = r1 - l2_soft[None, :] * r1
+    n0, n1 = xhat.shape[1:]
+    return v1, wv.sara_synthesis(v1, n0, n1, nlevel)
+
+
+def nuclear_prox_update(v0, xhat_facet, window, weights0, beta0):
+    """src/fhs/fhs_update_dual_lowrankness.m:40-45 (window = 1 gives
+    src/hs/hs_update_dual_lowrankness_serial.m:37-42 without sigma0).
+    v0 [P, L]; xhat_facet [L, ny, nx]; returns (v0, g0 [L, ny, nx])."""
+    L, ny, nx = xhat_facet.shape
+    Z = v0 + (window[None] * xhat_facet).reshape(L, -1).T
+    U, S, Vt = np.linalg.svd(Z, full_matrices=False)
+    v0 = Z - (U * np.maximum(S - beta0 * weights0, 0.0)) @ Vt
+    g0 = window[None] * v0.T.reshape(L, ny, nx)
+    return v0, g0
+
+
+def nuclear_weights(x_facet_weighted, sig_bar, alpha):
+    """src/fhs/fhs_update_weights.m:73-77: weights0 = u/(u + sigma_i)."""
+    L = x_facet_weighted.shape[0]
+    s = np.linalg.svd(x_facet_weighted.reshape(L, -1).T, compute_uv=False)
+    u = sig_bar * alpha
+    return u / (u + np.abs(s))
+
+
+def l21_weights(x, sig, alpha, nlevel=4):
+    """src/fhs/fhs_update_weights.m:79-92 (global coefficients)."""
+    z = wv.sara_analysis(x, nlevel)
+    d = np.sqrt(np.sum(z * z, axis=0))
+    u = sig * alpha
+    return u / (u + d)
+
+
+def compute_noise_level(Ny, Nx, L, std_noise, algo, geometry: FacetGeometry | None,
+                        squared_operator_norm):
+    """src/heuristics/compute_noise_level.m:49-89."""
+    std_noise = np.asarray(std_noise, dtype=np.float64)
+    son = np.asarray(squared_operator_norm, dtype=np.float64)
+    sig_sara = np.sqrt(np.mean(std_noise ** 2 / son))
+    mu_chi = np.sqrt(2.0) * np.exp(gammaln((L + 1) / 2.0) - gammaln(L / 2.0))
+    sig_chi = np.sqrt(L - mu_chi ** 2)
+    sig = sig_sara * (mu_chi + sig_chi)
+    s = np.sum(std_noise ** 2 / son)
+    if algo == "hs" or geometry is None:
+        sig_bar = np.sqrt(Nx * Ny * s / min(Nx * Ny, L))
+    else:
+        sig_bar = np.array([np.sqrt(geometry.n_pixels(q) * s / min(geometry.n_pixels(q), L))
+                            for q in range(geometry.Q)])
+    return sig, sig_bar, mu_chi, sig_chi, sig_sara
+
+
+# ----------------------------------------------------------------- solvers
+@dataclass
+class SolverParams:
+    """The ``param`` struct fields the solvers read (imaging/imaging.m:839-860,
+    imaging/default_parameters.json)."""
+    nu0: float = 1.0
+    nu1: float = 1.0
+    nu2: np.ndarray = None
+    gamma: float = 1e-3          # mu (l21 / l1)
+    gamma0: np.ndarray = None    # mu_bar per facet (or scalar for hs)
+    reweighting_sig: float = 1.0
+    reweighting_sig_bar: np.ndarray = None
+    reweighting_alpha: float = 1.0
+    reweighting_flag: bool = True
+    reweighting_min_iter: int = 1
+    reweighting_max_iter: int = 20
+    reweighting_rel_var: float = 1e-4
+    pdfb_min_iter: int = 10
+    pdfb_max_iter: int = 2000
+    pdfb_rel_var: float = 5e-5
+    pdfb_fidelity_tolerance: float = 1.01
+    pdfb_rel_var_low: float = 5e-6
+    nlevel: int = 4
+
+
+@dataclass
+class SolverLog:
+    rel_val: list = field(default_factory=list)
+    residual: list = field(default_factory=list)
+    epsilon: list = field(default_factory=list)
+    n_iter: int = 0
+    n_reweights: int = 0
+
+
+def _stop_pdfb(t, last, rel, res, epsn, p: SolverParams):
+    """src/fhs/facetHyperSARA.m:877-881."""
+    return (t - last >= p.pdfb_min_iter) and (
+        t - last >= p.pdfb_max_iter
+        or (rel <= p.pdfb_rel_var and res <= p.pdfb_fidelity_tolerance * epsn)
+        or rel <= p.pdfb_rel_var_low)
+
+
+def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
+                    xinit=None, max_iter=None, callback=None):
+    """src/fhs/facetHyperSARA.m:701-1138 (one spectral sub-cube, pU = 1)."""
+    op = data.op
+    L = data.L
+    x = np.zeros((L, op.Ny, op.Nx)) if xinit is None else np.array(xinit, dtype=np.float64)
+    tau = 0.99 / 3.0
+    sigma0, sigma1 = 1.0 / p.nu0, 1.0 / p.nu1
+    sigma00, sigma11 = tau * sigma0, tau * sigma1
+    sigma22 = tau / np.asarray(p.nu2, dtype=np.float64)
+    beta0 = np.asarray(p.gamma0, dtype=np.float64) / sigma0 * np.ones(geom.Q)
+    beta1 = p.gamma / sigma1
+    sig_bar = np.asarray(p.reweighting_sig_bar, dtype=np.float64) * np.ones(geom.Q)
+    facets = list(geom.facets())
+    # fhs_initialize_dual_and_weights.m:88-118
+    v0, w0 = [], []
+    zero = np.linalg.norm(x) == 0
+    for q, (y0, y1), (x0, x1), win in facets:
+        v0.append(np.zeros(((y1 - y0) * (x1 - x0), L)))
+        w0.append(np.ones(L) if zero else
+                  nuclear_weights(win[None] * x[:, y0:y1, x0:x1], sig_bar[q], p.reweighting_alpha))
+    s = wv.n_coefs_sara(op.Ny, op.Nx, p.nlevel)
+    v1 = np.zeros((L, s))
+    w1 = np.ones(s) if zero else l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
+    v2 = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
+    Fx_old = np.stack([op.A(x[l]) for l in range(L)])
+    g = np.zeros_like(x)
+    log = SolverLog()
+    x_last_rw = x.copy()
+    last, rw_count = 0, 0
+    max_iter = max_iter or (p.reweighting_max_iter + 1) * p.pdfb_max_iter
+    for t in range(1, max_iter + 1):
+        x, xhat, rel_x, norm_x = primal_update(x, g)
+        v2, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, sigma22)
+        gacc = np.zeros_like(x)
+        for q, (y0, y1), (x0, x1), win in facets:
+            v0[q], g0 = nuclear_prox_update(v0[q], xhat[:, y0:y1, x0:x1], win, w0[q], beta0[q])
+            gacc[:, y0:y1, x0:x1] += sigma00 * g0
+        v1, g1 = l21_prox_update(v1, xhat, w1, beta1, p.nlevel)
+        g = gacc + sigma11 * g1 + Ftx
+        rel = np.sqrt(rel_x / norm_x) if norm_x > 0 else 0.0
+        res, epsn = np.sqrt(gres), np.sqrt(geps)
+        log.rel_val.append(rel)
+        log.residual.append(res)
+        log.epsilon.append(epsn)
+        log.n_iter = t
+        if callback is not None:
+            callback(t, x)
+        if _stop_pdfb(t, last, rel, res, epsn, p):
+            rel_rw = np.linalg.norm(x_last_rw - x) / max(np.linalg.norm(x_last_rw), 1e-300)
+            if (not p.reweighting_flag) or (rw_count >= p.reweighting_min_iter and (
+                    rw_count >= p.reweighting_max_iter or rel_rw <= p.reweighting_rel_var)):
+                break
+            for q, (y0, y1), (x0, x1), win in facets:
+                w0[q] = nuclear_weights(win[None] * x[:, y0:y1, x0:x1], sig_bar[q], p.reweighting_alpha)
+            w1 = l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
+            x_last_rw = x.copy()
+            rw_count += 1
+            last = t
+    log.n_reweights = rw_count
+    return x, log
+
+
+def hypersara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None):
+    """src/hs/hyperSARA.m:565-866 (no faceting, pU = 1)."""
+    op = data.op
+    geom = FacetGeometry(op.Ny, op.Nx, 1, 1, (0, 0), window_type="none")
+    # HyperSARA is the Q = 1 faceted iteration without window; its g0 scaling
+    # (sigma0 inside hs_update_dual_lowrankness_serial.m:42) equals sigma00
+    # because hyperSARA.m:476 also builds sigma00 = tau*sigma0.
+    return facet_hypersara(data, p, geom, xinit, max_iter, callback)
+
+
+def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None):
+    """src/sara/sara.m:521-837 (single channel, per-basis l1 prox)."""
+    op = data.op
+    assert data.L == 1
+    x = np.zeros((1, op.Ny, op.Nx)) if xinit is None else np.array(xinit, dtype=np.float64).reshape(1, op.Ny, op.Nx)
+    sigma1 = 1.0 / p.nu1
+    sigma2 = 1.0 / float(np.asarray(p.nu2).ravel()[0])
+    tau = 0.99 / (sigma1 * p.nu1 + sigma2 * float(np.asarray(p.nu2).ravel()[0]))
+    sigma11, sigma22 = tau * sigma1, tau * sigma2
+    beta1 = p.gamma / sigma1
+    u = p.reweighting_sig * p.reweighting_alpha
+    w1 = u / (u + np.abs(wv.sara_analysis(x[0], p.nlevel)))      # sara.m:352-362
+    v1 = np.zeros_like(w1)
+    v2 = [[np.zeros_like(yb) for yb in data.y[0]]]
+    Fx_old = np.stack([op.A(x[0])])
+    g = np.zeros_like(x)
+    log = SolverLog()
+    x_last_rw = x.copy()
+    last, rw_count = 0, 0
+    max_iter = max_iter or (p.reweighting_max_iter + 1) * p.pdfb_max_iter
+    for t in range(1, max_iter + 1):
+        x, xhat, rel_x, norm_x = primal_update(x, g)
+        r1 = v1 + wv.sara_analysis(xhat[0], p.nlevel)                # run_par_waverec
+        v1 = r1 - np.sign(r1) * np.maximum(np.abs(r1) - beta1 * w1, 0.0)
+        g1 = wv.sara_synthesis(v1, op.Ny, op.Nx, p.nlevel)
+        v2, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, [1.0])
+        g = sigma11 * g1[None] + sigma22 * Ftx                        # sara.m:633
+        rel = np.sqrt(rel_x / norm_x) if norm_x > 0 else 0.0
+        res, epsn = np.sqrt(gres), np.sqrt(geps)
+        log.rel_val.append(rel)
+        log.residual.append(res)
+        log.epsilon.append(epsn)
+        log.n_iter = t
+        if callback is not None:
+            callback(t, x)
+        if _stop_pdfb(t, last, rel, res, epsn, p):
+            rel_rw = np.linalg.norm(x_last_rw - x) / max(np.linalg.norm(x_last_rw), 1e-300)
+            if (not p.reweighting_flag) or (rw_count >= p.reweighting_min_iter and (
+                    rw_count >= p.reweighting_max_iter or rel_rw <= p.reweighting_rel_var)):
+                break
+            w1 = u / (u + np.abs(wv.sara_analysis(x[0], p.nlevel)))   # sara.m:764-768
+            x_last_rw = x.copy()
+            rw_count += 1
+            last = t
+    log.n_reweights = rw_count
+    return x[0], log
+
+
+def snr_db(x_true, x):
+    return 20.0 * np.log10(np.linalg.norm(x_true) / np.linalg.norm(x_true - x))
