@@ -14,6 +14,11 @@
 // then a function of the fractional grid offset only and is read from a
 // 1024-sample table (linear interpolation, < 2e-7 relative error).
 //
+// The l2-ball dual takes two passes because the block norm ||z_b|| is a
+// reduction over all of a block's visibilities: pass 1 writes z to a scratch
+// buffer (zbuf) that pass 2 reads while the owner tile writes v2 = z*scale, so
+// CTAs that read a neighbour's visibilities never see a half-updated v2.
+//
 // Degridding: one CTA per 64x64 grid tile stages the tile and its (J-1)-cell
 // apron in shared memory and gathers the taps of the visibilities that start
 // in the tile.  Gridding: one CTA per tile accumulates, in shared memory, the
@@ -67,10 +72,10 @@ __device__ __forceinline__ int wrap(int k, int K) {
 // ---------------------------------------------------------------- degrid
 template <int J, bool DUAL>
 __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid, int c0,
-                                                     float2* __restrict__ out, float2* __restrict__ v2,
+                                                     float2* __restrict__ out, const float2* __restrict__ v2,
                                                      float2* __restrict__ gold,
                                                      const float2* __restrict__ y,
-                                                     double* __restrict__ partials) {
+                                                     double* __restrict__ partials, float2* __restrict__ zbuf) {
   __shared__ float2 sm[(kTileCells + J - 1) * (kTileCells + J - 1)];
   __shared__ double bacc[kMaxBlocksPerChannel * 2];
   constexpr int P = kTileCells + J - 1;
@@ -123,7 +128,7 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
       const float2 go = gold[vo + i];
       const float2 z = make_float2(vv.x + 2.f * gfx.x - go.x - yv.x, vv.y + 2.f * gfx.y - go.y - yv.y);
       const float2 r = make_float2(gfx.x - yv.x, gfx.y - yv.y);
-      v2[vo + i] = z;
+      zbuf[vo + i] = z;
       gold[vo + i] = gfx;
       const int blk = (int)(kp >> 28);
       atomicAdd(&bacc[2 * blk], (double)z.x * z.x + (double)z.y * z.y);
@@ -153,7 +158,8 @@ template <int J, bool DUAL>
 __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict__ gridB, int c0,
                                                    const float2* __restrict__ vin,
                                                    float2* __restrict__ v2,
-                                                   const float* __restrict__ blk_scale) {
+                                                   const float* __restrict__ blk_scale,
+                                                   const float2* __restrict__ zbuf) {
   __shared__ float acc_re[kTileCells * kTileCells];
   __shared__ float acc_im[kTileCells * kTileCells];
   __shared__ Range rng[2 + 2 * kSubPerTile];
@@ -214,7 +220,7 @@ __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict
     const bool own = (r == 0);
     float2 v;
     if (DUAL) {
-      const float2 z = v2[vo + i];
+      const float2 z = zbuf[vo + i];
       const float sc = scl[kp >> 28];
       v = make_float2(z.x * sc, z.y * sc);
       if (own) v2[vo + i] = v;
@@ -500,6 +506,7 @@ void measop_commit(MeasOp* op) {
   upload_table(op->ay, op->tab_y, op->sy);
   upload_table(op->ax, op->tab_x, op->sx);
   op->geom.alloc(std::max<int64_t>(op->Mtot, 1));
+  op->zbuf.alloc(std::max<int64_t>(op->Mtot, 1));
   op->perm.alloc(std::max<int64_t>(op->Mtot, 1));
   op->sb_off.alloc((size_t)L * (op->nkeys + 1));
   for (int c = 0; c < L; ++c) {
@@ -577,14 +584,14 @@ void fft_inverse(const MeasOp* op, int p0, int np, cudaStream_t s) {
 void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s) {
   dim3 grid(op->ntiles(), nc);
   degrid_kernel<7, false><<<grid, 256, 0, s>>>(op->view(), op->gridA.p, c0, out, nullptr, nullptr, nullptr,
-                                               nullptr);
+                                               nullptr, nullptr);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
 
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s) {
   dim3 grid(op->ntiles(), nc);
-  grid_kernel<7, false><<<grid, 256, 0, s>>>(op->view(), op->gridB.p, c0, v, nullptr, nullptr);
+  grid_kernel<7, false><<<grid, 256, 0, s>>>(op->view(), op->gridB.p, c0, v, nullptr, nullptr, nullptr);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
@@ -601,7 +608,7 @@ void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* go
                         cudaStream_t s) {
   dim3 grid(op->ntiles(), nc);
   degrid_kernel<7, true><<<grid, 256, 0, s>>>(op->view(), op->gridA.p, c0, nullptr, v2, gold, y,
-                                              op->partials.p);
+                                              op->partials.p, op->zbuf.p);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
@@ -616,7 +623,8 @@ void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s) {
 
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s) {
   dim3 grid(op->ntiles(), nc);
-  grid_kernel<7, true><<<grid, 256, 0, s>>>(op->view(), op->gridB.p, c0, nullptr, v2, op->blk_scale.p);
+  grid_kernel<7, true><<<grid, 256, 0, s>>>(op->view(), op->gridB.p, c0, nullptr, v2, op->blk_scale.p,
+                                            op->zbuf.p);
   count_launch();
   FHS_LAUNCH_CHECK();
 }

@@ -52,6 +52,7 @@ struct MeasOp {
   DevBuf<float2> tab_y, tab_x;
   DevBuf<float> sy, sx;
   DevBuf<float4> geom;
+  DevBuf<float2> zbuf;      // pass-1 output z of the l2-ball dual update
   DevBuf<int32_t> perm;
   DevBuf<int32_t> sb_off;
   DevBuf<int64_t> ch_voff;
@@ -95,12 +96,12 @@ void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStre
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
 // out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1
 void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s);
-// fused dual update, pass 1: GFx, z -> v2, GFx -> gold, block partials
+// fused dual update, pass 1: GFx, z = v2 + 2 GFx - gold - y -> zbuf, GFx -> gold, block partials
 void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
                         cudaStream_t s);
 // block reduction: scale = 1 - min(eps/||z||, 1); stats for the report
 void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s);
-// fused dual update, pass 2: v2 <- z*scale, gridB <- G^H v2
+// fused dual update, pass 2: v2 <- zbuf*scale, gridB <- G^H v2
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s);
 
 }  // namespace fhs

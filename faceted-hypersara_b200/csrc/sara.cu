@@ -1,0 +1,541 @@
+// SARA dictionary and weighted l21 prox on B200 (sm_100a).
+//
+// Replaces op_p_sp_wlt_basis / sdwt2_sara_faceting / isdwt2_sara_faceting of
+// the SARA-dictionary submodule (called at imaging/imaging.m:802 and
+// src/fhs/fhs_update_dual_sparsity.m:75,92) and the l21 prox of
+// src/fhs/fhs_update_dual_sparsity.m:84-89 /
+// src/hs/hs_update_dual_sparsity_distributed.m:41-54.
+//
+// Daubechies db1..db8 extremal-phase filters are computed on the host by
+// spectral factorisation (Daubechies, Ten Lectures, sec. 6.1) in FP64.  One
+// analysis level filters a 2-D tile along x then y (zero padding, full
+// convolution, odd samples kept) and writes the four subbands in MATLAB's
+// wavedec2 layout; one synthesis level is the exact adjoint.  All 8 bases and
+// all channels of a level run in one launch.  The faceted transform of the
+// reference produces the same coefficients as this global transform
+// (segmentwise DWT, Prusa 2012), split over facets.
+#include "sara.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+
+namespace fhs {
+
+namespace {
+
+__constant__ float c_lo[kSaraWavelets][kSaraMaxFilter];  // Lo_D
+__constant__ float c_hi[kSaraWavelets][kSaraMaxFilter];  // Hi_D
+
+// ------------------------------------------------------------- filters
+std::vector<double> poly_mul(const std::vector<double>& a, const std::vector<double>& b) {
+  std::vector<double> c(a.size() + b.size() - 1, 0.0);
+  for (size_t i = 0; i < a.size(); ++i)
+    for (size_t j = 0; j < b.size(); ++j) c[i + j] += a[i] * b[j];
+  return c;
+}
+
+// Roots of a real polynomial (coefficients highest degree first) by the
+// Durand-Kerner iteration followed by Newton polishing.
+std::vector<std::complex<double>> poly_roots(const std::vector<double>& c) {
+  const int n = (int)c.size() - 1;
+  std::vector<std::complex<double>> r(n);
+  if (n <= 0) return r;
+  auto eval = [&](std::complex<double> z) {
+    std::complex<double> v = c[0];
+    for (int i = 1; i <= n; ++i) v = v * z + c[i];
+    return v;
+  };
+  auto deriv = [&](std::complex<double> z) {
+    std::complex<double> v = c[0] * (double)n;
+    for (int i = 1; i < n; ++i) v = v * z + c[i] * (double)(n - i);
+    return v;
+  };
+  const std::complex<double> seed(0.4, 0.9);
+  for (int i = 0; i < n; ++i) r[i] = std::pow(seed, i);
+  for (int it = 0; it < 2000; ++it) {
+    double delta = 0;
+    for (int i = 0; i < n; ++i) {
+      std::complex<double> den = c[0];
+      for (int j = 0; j < n; ++j)
+        if (j != i) den *= (r[i] - r[j]);
+      const std::complex<double> d = eval(r[i]) / den;
+      r[i] -= d;
+      delta = std::max(delta, std::abs(d));
+    }
+    if (delta < 1e-15) break;
+  }
+  for (auto& z : r)
+    for (int k = 0; k < 5; ++k) {
+      const auto d = deriv(z);
+      if (std::abs(d) > 0) z -= eval(z) / d;
+    }
+  return r;
+}
+
+// Extremal-phase Daubechies scaling filter with p vanishing moments, oriented
+// as MATLAB's reconstruction low-pass Lo_R, normalised to sum sqrt(2).
+std::vector<double> daubechies(int p) {
+  std::vector<double> h;
+  if (p == 1) return {1.0 / std::sqrt(2.0), 1.0 / std::sqrt(2.0)};
+  // z^{p-1} P((2 - z - 1/z)/4) with P(y) = sum_k C(p-1+k, k) y^k
+  const std::vector<double> base = {-0.25, 0.5, -0.25};
+  std::vector<double> poly(2 * p - 1, 0.0);
+  for (int k = 0; k < p; ++k) {
+    double ck = 1.0;
+    for (int i = 1; i <= k; ++i) ck = ck * (p - 1 + i) / i;
+    std::vector<double> term = {1.0};
+    for (int i = 0; i < k; ++i) term = poly_mul(term, base);
+    term.resize(term.size() + (p - 1 - k), 0.0);
+    const size_t off = poly.size() - term.size();
+    for (size_t i = 0; i < term.size(); ++i) poly[off + i] += ck * term[i];
+  }
+  const auto roots = poly_roots(poly);
+  std::vector<std::complex<double>> q = {1.0};
+  for (const auto& z : roots) {
+    if (std::abs(z) >= 1.0) continue;
+    std::vector<std::complex<double>> nq(q.size() + 1, 0.0);
+    for (size_t i = 0; i < q.size(); ++i) {
+      nq[i] += q[i];
+      nq[i + 1] -= q[i] * z;
+    }
+    q = nq;
+  }
+  h.resize(q.size());
+  for (size_t i = 0; i < q.size(); ++i) h[i] = q[i].real();
+  for (int i = 0; i < p; ++i) h = poly_mul(h, {1.0, 1.0});
+  double sum = 0;
+  for (double v : h) sum += v;
+  for (double& v : h) v = v / sum * std::sqrt(2.0);
+  return h;
+}
+
+bool g_filters_ready[64] = {false};
+
+void upload_filters() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && g_filters_ready[dev]) return;
+  float lo[kSaraWavelets][kSaraMaxFilter] = {};
+  float hi[kSaraWavelets][kSaraMaxFilter] = {};
+  for (int b = 0; b < kSaraWavelets; ++b) {
+    const std::vector<double> lo_r = daubechies(b + 1);
+    const int L = (int)lo_r.size();
+    for (int k = 0; k < L; ++k) lo[b][k] = (float)lo_r[L - 1 - k];  // Lo_D = reverse(Lo_R)
+    // Hi_D = reverse(Hi_R): Hi_D[k] = Hi_R[L-1-k] = (-1)^(L-1-k) Lo_R[k]
+    for (int k = 0; k < L; ++k) hi[b][k] = (float)((((L - 1 - k) % 2) ? -1.0 : 1.0) * lo_r[k]);
+  }
+  FHS_CUDA(cudaMemcpyToSymbol(c_lo, lo, sizeof(lo)));
+  FHS_CUDA(cudaMemcpyToSymbol(c_hi, hi, sizeof(hi)));
+  if (dev < 64) g_filters_ready[dev] = true;
+}
+
+// ------------------------------------------------------------ analysis
+constexpr int AT0 = 32, AT1 = 8;                 // output tile (y, x)
+constexpr int AIN0 = 2 * AT0 + kSaraMaxFilter - 2;  // 78
+constexpr int AIN1 = 2 * AT1 + kSaraMaxFilter - 2;  // 30
+
+struct LevelArgs {
+  int n0[kSaraWavelets], n1[kSaraWavelets];   // input sizes
+  int m0[kSaraWavelets], m1[kSaraWavelets];   // output sizes
+  int tiles0[kSaraWavelets], tiles[kSaraWavelets];
+  int64_t in_off[kSaraWavelets];
+  int64_t a_off[kSaraWavelets];
+  int64_t h_off[kSaraWavelets];
+  int64_t in_stride, s_stride, apx_stride;
+  int first, last;   // input from x (level 1); A into coef (level J)
+  float in_scale;
+};
+
+__global__ void __launch_bounds__(256) analysis_kernel(LevelArgs a, const float* __restrict__ x,
+                                                       float* __restrict__ coef, float* __restrict__ apx) {
+  __shared__ float sin_[AIN1][AIN0 + 1];
+  __shared__ float tlo[AT1][AIN0 + 1];
+  __shared__ float thi[AT1][AIN0 + 1];
+  const int b = blockIdx.y;
+  const int plane = blockIdx.z;
+  const int tile = blockIdx.x;
+  if (tile >= a.tiles[b]) return;
+  const int Lf = 2 * (b + 1);
+  const int n0 = a.n0[b], n1 = a.n1[b], m0 = a.m0[b], m1 = a.m1[b];
+  const int tp0 = tile % a.tiles0[b], tp1 = tile / a.tiles0[b];
+  const int p0s = tp0 * AT0, p1s = tp1 * AT1;
+  const int i0s = 2 * p0s + 2 - Lf, i1s = 2 * p1s + 2 - Lf;
+  const int IN0 = 2 * AT0 + Lf - 2, IN1 = 2 * AT1 + Lf - 2;
+  const float* src = a.first ? x + (size_t)plane * a.in_stride
+                             : apx + (size_t)plane * a.apx_stride + a.in_off[b];
+  for (int idx = threadIdx.x; idx < IN0 * IN1; idx += blockDim.x) {
+    const int l1 = idx / IN0, l0 = idx - l1 * IN0;
+    const int i0 = i0s + l0, i1 = i1s + l1;
+    float v = 0.f;
+    if (i0 >= 0 && i0 < n0 && i1 >= 0 && i1 < n1) v = src[(size_t)i1 * n0 + i0] * a.in_scale;
+    sin_[l1][l0] = v;
+  }
+  __syncthreads();
+  // filter along x (dim 2): tlo/thi[p1][i0]
+  for (int idx = threadIdx.x; idx < AT1 * IN0; idx += blockDim.x) {
+    const int lp1 = idx / IN0, l0 = idx - lp1 * IN0;
+    float lo = 0.f, hi = 0.f;
+    for (int t = 0; t < Lf; ++t) {
+      const float v = sin_[2 * lp1 + Lf - 1 - t][l0];
+      lo = fmaf(c_lo[b][t], v, lo);
+      hi = fmaf(c_hi[b][t], v, hi);
+    }
+    tlo[lp1][l0] = lo;
+    thi[lp1][l0] = hi;
+  }
+  __syncthreads();
+  const int lp0 = threadIdx.x % AT0, lp1 = threadIdx.x / AT0;
+  const int p0 = p0s + lp0, p1 = p1s + lp1;
+  if (lp1 < AT1 && p0 < m0 && p1 < m1) {
+    float aa = 0.f, hh = 0.f, vv = 0.f, dd = 0.f;
+    for (int t = 0; t < Lf; ++t) {
+      const int l0 = 2 * lp0 + Lf - 1 - t;
+      const float lo = tlo[lp1][l0], hi = thi[lp1][l0];
+      aa = fmaf(c_lo[b][t], lo, aa);
+      hh = fmaf(c_hi[b][t], lo, hh);
+      vv = fmaf(c_lo[b][t], hi, vv);
+      dd = fmaf(c_hi[b][t], hi, dd);
+    }
+    const size_t o = (size_t)p1 * m0 + p0;
+    const size_t mm = (size_t)m0 * m1;
+    float* cp = coef + (size_t)plane * a.s_stride + a.h_off[b];
+    cp[o] = hh;
+    cp[mm + o] = vv;
+    cp[2 * mm + o] = dd;
+    if (a.last)
+      coef[(size_t)plane * a.s_stride + a.a_off[b] + o] = aa;
+    else
+      apx[(size_t)plane * a.apx_stride + a.a_off[b] + o] = aa;
+  }
+}
+
+// ----------------------------------------------------------- synthesis
+constexpr int ST0 = 32, ST1 = 16;                          // output tile (y, x)
+constexpr int SP0 = ST0 / 2 + kSaraMaxFilter / 2;          // 24 coefficient rows
+constexpr int SP1 = ST1 / 2 + kSaraMaxFilter / 2;          // 16
+
+struct SynArgs {
+  int m0[kSaraWavelets], m1[kSaraWavelets];    // coefficient sizes (level j)
+  int n0[kSaraWavelets], n1[kSaraWavelets];    // output sizes (level j-1)
+  int tiles0[kSaraWavelets], tiles[kSaraWavelets];
+  int64_t a_off[kSaraWavelets];                // A_j (coef if from_coef, else apx)
+  int64_t h_off[kSaraWavelets];                // H_j in coef
+  int64_t out_off[kSaraWavelets];              // level j-1 approximation in apx
+  int64_t s_stride, apx_stride, out_stride;
+  int a_from_coef;
+  int final_level;                             // j == 1: sum bases + Dirac into out
+  int64_t dirac_off;
+  float alpha;
+};
+
+// Accumulates the synthesis of basis b for the output tile into acc[2].
+__device__ __forceinline__ void syn_basis(const SynArgs& a, int b, int plane, const float* __restrict__ coef,
+                                          const float* __restrict__ apx, int I0s, int I1s,
+                                          float (*sub)[SP1][SP0], float (*tlo)[ST0], float (*thi)[ST0],
+                                          float acc[2]) {
+  const int Lf = 2 * (b + 1);
+  const int m0 = a.m0[b], m1 = a.m1[b];
+  const int P0s = I0s / 2, P1s = I1s / 2;
+  const int P0n = (I0s + ST0 - 1 + Lf - 2) / 2 - P0s + 1;
+  const int P1n = (I1s + ST1 - 1 + Lf - 2) / 2 - P1s + 1;
+  const float* A = (a.a_from_coef ? coef + (size_t)plane * a.s_stride : apx + (size_t)plane * a.apx_stride) +
+                   a.a_off[b];
+  const float* H = coef + (size_t)plane * a.s_stride + a.h_off[b];
+  const size_t mm = (size_t)m0 * m1;
+  for (int idx = threadIdx.x; idx < P0n * P1n; idx += blockDim.x) {
+    const int l1 = idx / P0n, l0 = idx - l1 * P0n;
+    const int p0 = P0s + l0, p1 = P1s + l1;
+    float va = 0.f, vh = 0.f, vv = 0.f, vd = 0.f;
+    if (p0 < m0 && p1 < m1) {
+      const size_t o = (size_t)p1 * m0 + p0;
+      va = A[o];
+      vh = H[o];
+      vv = H[mm + o];
+      vd = H[2 * mm + o];
+    }
+    sub[0][l1][l0] = va;
+    sub[1][l1][l0] = vh;
+    sub[2][l1][l0] = vv;
+    sub[3][l1][l0] = vd;
+  }
+  __syncthreads();
+  // along y: tlo/thi[p1][i0]
+  for (int idx = threadIdx.x; idx < P1n * ST0; idx += blockDim.x) {
+    const int l1 = idx / ST0, li0 = idx - l1 * ST0;
+    const int i0 = I0s + li0;
+    float lo = 0.f, hi = 0.f;
+    const int pa = i0 / 2, pb = (i0 + Lf - 2) / 2;
+    for (int p0 = pa; p0 <= pb; ++p0) {
+      const int t = 2 * p0 + 1 - i0;
+      const int l0 = p0 - P0s;
+      lo = fmaf(sub[0][l1][l0], c_lo[b][t], fmaf(sub[1][l1][l0], c_hi[b][t], lo));
+      hi = fmaf(sub[2][l1][l0], c_lo[b][t], fmaf(sub[3][l1][l0], c_hi[b][t], hi));
+    }
+    tlo[l1][li0] = lo;
+    thi[l1][li0] = hi;
+  }
+  __syncthreads();
+  const int li0 = threadIdx.x % ST0;
+  for (int r = 0; r < 2; ++r) {
+    const int li1 = threadIdx.x / ST0 + 8 * r;
+    const int i1 = I1s + li1;
+    float v = 0.f;
+    const int pa = i1 / 2, pb = (i1 + Lf - 2) / 2;
+    for (int p1 = pa; p1 <= pb; ++p1) {
+      const int t = 2 * p1 + 1 - i1;
+      v = fmaf(tlo[p1 - P1s][li0], c_lo[b][t], fmaf(thi[p1 - P1s][li0], c_hi[b][t], v));
+    }
+    acc[r] += v;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
+                                                        float* __restrict__ apx, float* __restrict__ out) {
+  __shared__ float sub[4][SP1][SP0];
+  __shared__ float tlo[SP1][ST0];
+  __shared__ float thi[SP1][ST0];
+  const int plane = blockIdx.z;
+  const int tile = blockIdx.x;
+  if (!a.final_level) {
+    const int b = blockIdx.y;
+    if (tile >= a.tiles[b]) return;
+    const int ti0 = tile % a.tiles0[b], ti1 = tile / a.tiles0[b];
+    const int I0s = ti0 * ST0, I1s = ti1 * ST1;
+    float acc[2] = {0.f, 0.f};
+    syn_basis(a, b, plane, coef, apx, I0s, I1s, sub, tlo, thi, acc);
+    const int n0 = a.n0[b], n1 = a.n1[b];
+    const int li0 = threadIdx.x % ST0;
+    for (int r = 0; r < 2; ++r) {
+      const int i0 = I0s + li0, i1 = I1s + threadIdx.x / ST0 + 8 * r;
+      if (i0 < n0 && i1 < n1) apx[(size_t)plane * a.apx_stride + a.out_off[b] + (size_t)i1 * n0 + i0] = acc[r];
+    }
+    return;
+  }
+  // final level: all bases share the output size (the image)
+  const int n0 = a.n0[0], n1 = a.n1[0];
+  if (tile >= a.tiles[0]) return;
+  const int ti0 = tile % a.tiles0[0], ti1 = tile / a.tiles0[0];
+  const int I0s = ti0 * ST0, I1s = ti1 * ST1;
+  float acc[2] = {0.f, 0.f};
+  for (int b = 0; b < kSaraWavelets; ++b) syn_basis(a, b, plane, coef, apx, I0s, I1s, sub, tlo, thi, acc);
+  const int li0 = threadIdx.x % ST0;
+  for (int r = 0; r < 2; ++r) {
+    const int i0 = I0s + li0, i1 = I1s + threadIdx.x / ST0 + 8 * r;
+    if (i0 < n0 && i1 < n1) {
+      const size_t o = (size_t)i1 * n0 + i0;
+      const float dirac = coef[(size_t)plane * a.s_stride + a.dirac_off + o];
+      out[(size_t)plane * a.out_stride + o] = a.alpha * (acc[r] + dirac);
+    }
+  }
+}
+
+// ------------------------------------------------------------- prox
+template <int MAXL>
+__global__ void __launch_bounds__(256) l21_prox_kernel(float* __restrict__ v1, const float* __restrict__ coef,
+                                                       const float* __restrict__ xhat,
+                                                       const float* __restrict__ weights,
+                                                       const double* __restrict__ beta, int64_t s,
+                                                       int64_t dirac_off, int64_t npix, int lg,
+                                                       double* __restrict__ l21_partials) {
+  const int g = blockIdx.y;
+  const float bt = (float)beta[g];
+  const float* wg = weights + (size_t)g * s;
+  double l21 = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (int64_t)gridDim.x * blockDim.x) {
+    float w[MAXL];
+    float ss = 0.f;
+#pragma unroll
+    for (int l = 0; l < MAXL; ++l) {
+      if (l < lg) {
+        const size_t plane = (size_t)g * lg + l;
+        const float c = i < dirac_off ? coef[plane * s + i] : xhat[plane * npix + (i - dirac_off)] * (1.f / 3.f);
+        w[l] = v1[plane * s + i] + c;
+        ss = fmaf(w[l], w[l], ss);
+      }
+    }
+    const float l2 = sqrtf(ss);
+    l21 += l2;
+    const float soft = fmaxf(l2 - bt * wg[i], 0.f) / (l2 + 2.220446049250313e-16f);
+#pragma unroll
+    for (int l = 0; l < MAXL; ++l)
+      if (l < lg) v1[((size_t)g * lg + l) * s + i] = w[l] - soft * w[l];
+  }
+  if (l21_partials) {
+    __shared__ double red[256];
+    red[threadIdx.x] = l21;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+      if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) l21_partials[(size_t)g * gridDim.x + blockIdx.x] = red[0];
+  }
+}
+
+__global__ void row_norms_kernel(const float* __restrict__ coef, const float* __restrict__ x, int64_t s,
+                                 int64_t dirac_off, int64_t npix, int lg, float* __restrict__ out) {
+  const int g = blockIdx.y;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (int64_t)gridDim.x * blockDim.x) {
+    double ss = 0.0;
+    for (int l = 0; l < lg; ++l) {
+      const size_t plane = (size_t)g * lg + l;
+      const float c = i < dirac_off ? coef[plane * s + i] : x[plane * npix + (i - dirac_off)] * (1.f / 3.f);
+      ss += (double)c * c;
+    }
+    out[(size_t)g * s + i] = (float)sqrt(ss);
+  }
+}
+
+__global__ void dirac_kernel(const float* __restrict__ x, float* __restrict__ coef, int64_t s, int64_t off,
+                             int64_t npix) {
+  const int plane = blockIdx.y;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (int64_t)gridDim.x * blockDim.x)
+    coef[(size_t)plane * s + off + i] = x[(size_t)plane * npix + i] * (1.f / 3.f);
+}
+
+int nblk(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 8); }
+
+}  // namespace
+
+SaraPlan sara_plan(int Ny, int Nx, int J) {
+  FHS_CHECK(Ny > 0 && Nx > 0, FHS_ERR_INVALID_ARG, "bad image size");
+  FHS_CHECK(J >= 1 && J <= kSaraMaxLevel, FHS_ERR_UNSUPPORTED, "nlevel must be in [1, 8]");
+  SaraPlan p;
+  p.Ny = Ny;
+  p.Nx = Nx;
+  p.J = J;
+  int64_t pos = 0, apos = 0;
+  for (int b = 0; b < kSaraWavelets; ++b) {
+    const int Lf = 2 * (b + 1);
+    p.n0[b][0] = Ny;
+    p.n1[b][0] = Nx;
+    for (int j = 1; j <= J; ++j) {
+      p.n0[b][j] = (p.n0[b][j - 1] + Lf - 1) / 2;
+      p.n1[b][j] = (p.n1[b][j - 1] + Lf - 1) / 2;
+    }
+    p.boff[b] = pos;
+    p.offA[b] = pos;
+    pos += (int64_t)p.n0[b][J] * p.n1[b][J];
+    for (int j = J; j >= 1; --j) {
+      p.offH[b][j] = pos;
+      pos += 3 * (int64_t)p.n0[b][j] * p.n1[b][j];
+    }
+    for (int j = 1; j < J; ++j) {
+      p.apx_off[b][j] = apos;
+      apos += (int64_t)p.n0[b][j] * p.n1[b][j];
+    }
+  }
+  p.boff[kSaraWavelets] = pos;
+  pos += (int64_t)Ny * Nx;
+  p.s = pos;
+  p.apx_total = std::max<int64_t>(apos, 1);
+  return p;
+}
+
+void sara_analysis(const SaraPlan& p, const float* x, float* coef, float* apx, int np, cudaStream_t s) {
+  upload_filters();
+  for (int j = 1; j <= p.J; ++j) {
+    LevelArgs a{};
+    int maxt = 0;
+    for (int b = 0; b < kSaraWavelets; ++b) {
+      a.n0[b] = p.n0[b][j - 1];
+      a.n1[b] = p.n1[b][j - 1];
+      a.m0[b] = p.n0[b][j];
+      a.m1[b] = p.n1[b][j];
+      a.tiles0[b] = ceil_div(a.m0[b], AT0);
+      a.tiles[b] = a.tiles0[b] * ceil_div(a.m1[b], AT1);
+      maxt = std::max(maxt, a.tiles[b]);
+      a.in_off[b] = j > 1 ? p.apx_off[b][j - 1] : 0;
+      a.a_off[b] = j == p.J ? p.offA[b] : p.apx_off[b][j];
+      a.h_off[b] = p.offH[b][j];
+    }
+    a.in_stride = (int64_t)p.Ny * p.Nx;
+    a.s_stride = p.s;
+    a.apx_stride = p.apx_total;
+    a.first = j == 1;
+    a.last = j == p.J;
+    a.in_scale = j == 1 ? 1.f / 3.f : 1.f;
+    dim3 grid(maxt, kSaraWavelets, np);
+    analysis_kernel<<<grid, 256, 0, s>>>(a, x, coef, apx);
+    count_launch();
+    FHS_LAUNCH_CHECK();
+  }
+}
+
+void sara_dirac(const SaraPlan& p, const float* x, float* coef, int np, cudaStream_t s) {
+  const int64_t npix = (int64_t)p.Ny * p.Nx;
+  dirac_kernel<<<dim3(nblk(npix), np), 256, 0, s>>>(x, coef, p.s, p.boff[kSaraWavelets], npix);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
+void sara_synthesis(const SaraPlan& p, const float* coef, float* out, float* apx, int np, float alpha,
+                    cudaStream_t s) {
+  upload_filters();
+  for (int j = p.J; j >= 1; --j) {
+    SynArgs a{};
+    int maxt = 0;
+    for (int b = 0; b < kSaraWavelets; ++b) {
+      a.m0[b] = p.n0[b][j];
+      a.m1[b] = p.n1[b][j];
+      a.n0[b] = p.n0[b][j - 1];
+      a.n1[b] = p.n1[b][j - 1];
+      a.tiles0[b] = ceil_div(a.n0[b], ST0);
+      a.tiles[b] = a.tiles0[b] * ceil_div(a.n1[b], ST1);
+      maxt = std::max(maxt, a.tiles[b]);
+      a.a_off[b] = j == p.J ? p.offA[b] : p.apx_off[b][j];
+      a.h_off[b] = p.offH[b][j];
+      a.out_off[b] = j > 1 ? p.apx_off[b][j - 1] : 0;
+    }
+    a.s_stride = p.s;
+    a.apx_stride = p.apx_total;
+    a.out_stride = (int64_t)p.Ny * p.Nx;
+    a.a_from_coef = j == p.J;
+    a.final_level = j == 1;
+    a.dirac_off = p.boff[kSaraWavelets];
+    a.alpha = alpha / 3.f;
+    dim3 grid(a.final_level ? a.tiles[0] : maxt, a.final_level ? 1 : kSaraWavelets, np);
+    synthesis_kernel<<<grid, 256, 0, s>>>(a, coef, apx, out);
+    count_launch();
+    FHS_LAUNCH_CHECK();
+  }
+}
+
+void sara_l21_prox(const SaraPlan& p, float* v1, const float* coef, const float* xhat, const float* weights,
+                   const double* beta, int n_groups, int lg, double* l21_partials, cudaStream_t s) {
+  const int64_t npix = (int64_t)p.Ny * p.Nx;
+  dim3 grid(nblk(p.s), n_groups);
+  const int64_t off = p.boff[kSaraWavelets];
+#define FHS_L21(MAXL)                                                                                       \
+  l21_prox_kernel<MAXL><<<grid, 256, 0, s>>>(v1, coef, xhat, weights, beta, p.s, off, npix, lg, l21_partials)
+  if (lg <= 1)
+    FHS_L21(1);
+  else if (lg <= 4)
+    FHS_L21(4);
+  else if (lg <= 8)
+    FHS_L21(8);
+  else if (lg <= 16)
+    FHS_L21(16);
+  else if (lg <= 32)
+    FHS_L21(32);
+  else if (lg <= 64)
+    FHS_L21(64);
+  else
+    throw Error(FHS_ERR_UNSUPPORTED, "more than 64 channels per spectral group");
+#undef FHS_L21
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
+void sara_row_norms(const SaraPlan& p, const float* coef, const float* x, int n_groups, int lg, float* out,
+                    cudaStream_t s) {
+  const int64_t npix = (int64_t)p.Ny * p.Nx;
+  row_norms_kernel<<<dim3(nblk(p.s), n_groups), 256, 0, s>>>(coef, x, p.s, p.boff[kSaraWavelets], npix, lg,
+                                                              out);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
+}  // namespace fhs

@@ -1,0 +1,676 @@
+// Primal-dual iteration of facetHyperSARA / hyperSARA / sara on B200.
+//
+// One iteration (src/fhs/facetHyperSARA.m:701-783, src/hs/hyperSARA.m:565-617,
+// src/sara/sara.m:521-637) is a fixed launch sequence on one stream, captured
+// once into a CUDA graph and replayed:
+//   primal update + scaled zero-padded image for the FFT   (fhs_update_primal.m:33-38)
+//   FFT, degridding + l2-ball dual (pass 1), block norms,
+//   dual scaling + gridding (pass 2), inverse FFT          (update_dual_data_fidelity.m:116-147)
+//   SARA analysis of xhat, l21 prox, synthesis            (fhs_update_dual_sparsity.m:67-93)
+//   facet Gram, FP64 eigensolve, rank-L update            (fhs_update_dual_lowrankness.m:40-45)
+//   g = sigma00 sum_q D_q v0_q + sigma11 Psi v1 + sigma22 Re(At G^H v2)
+//   FP64 statistics into a device ring (rel_x, ||x||, residual, eps, priors).
+// The host reads the ring once per iteration only when it evaluates the
+// stopping rule (facetHyperSARA.m:877-881) and reweights (:952-1137).
+#include <chrono>
+#include <cmath>
+#include <memory>
+
+#include "apikern.cuh"
+#include "solver.cuh"
+
+namespace fhs {
+
+namespace {
+
+constexpr int kPrimalBlocks = 128;
+
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double sa[32], sb[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int w = threadIdx.x / 32, ln = threadIdx.x % 32;
+  if (ln == 0) {
+    sa[w] = a;
+    sb[w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x / 32;
+    a = ln < nw ? sa[ln] : 0.0;
+    b = ln < nw ? sb[ln] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, const float* __restrict__ g,
+                                                         float* __restrict__ xhat, float2* __restrict__ pad,
+                                                         const float* __restrict__ sy, const float* __restrict__ sx,
+                                                         int Ny, int Nx, int Ky, int Kx, double* __restrict__ part) {
+  const int plane = blockIdx.y;
+  const int64_t N = (int64_t)Ny * Nx;
+  float* xp = x + (size_t)plane * N;
+  const float* gp = g + (size_t)plane * N;
+  float* hp = xhat + (size_t)plane * N;
+  float2* pp = pad + (size_t)plane * Ky * Kx;
+  double a = 0.0, b = 0.0;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+    const float xo = xp[p];
+    const float xn = fmaxf(xo - gp[p], 0.f);
+    xp[p] = xn;
+    hp[p] = 2.f * xn - xo;
+    const double d = (double)xo - xn;
+    a += d * d;
+    b += (double)xn * xn;
+    const int ix = (int)(p / Ny), iy = (int)(p - (int64_t)ix * Ny);
+    int ky = iy - Ny / 2;
+    ky += ky < 0 ? Ky : 0;
+    int kx = ix - Nx / 2;
+    kx += kx < 0 ? Kx : 0;
+    pp[(size_t)kx * Ky + ky] = make_float2(xn * sy[iy] * sx[ix], 0.f);
+  }
+  block_sum2(a, b);
+  if (threadIdx.x == 0) {
+    part[((size_t)plane * gridDim.x + blockIdx.x) * 2] = a;
+    part[((size_t)plane * gridDim.x + blockIdx.x) * 2 + 1] = b;
+  }
+}
+
+struct AssembleArgs {
+  int Ny, Nx, Ky, Kx, lg, Qy, nuclear;
+  float sigma00;
+  const NucFacet* facets;
+  const float* wy;
+  const float* wx;
+  const int* cover_y;
+  const int* cover_x;
+  int64_t v0_group;
+};
+
+__global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, float* __restrict__ g,
+                                                       const float2* __restrict__ gridA, const float* __restrict__ g1,
+                                                       const float* __restrict__ v0, const float* __restrict__ sigma22,
+                                                       const float* __restrict__ sy, const float* __restrict__ sx) {
+  const int plane = blockIdx.y;
+  const int grp = plane / a.lg, lc = plane - grp * a.lg;
+  const int64_t N = (int64_t)a.Ny * a.Nx;
+  const float s22 = sigma22[plane];
+  const float2* gp = gridA + (size_t)plane * a.Ky * a.Kx;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(p / a.Ny), iy = (int)(p - (int64_t)ix * a.Ny);
+    int ky = iy - a.Ny / 2;
+    ky += ky < 0 ? a.Ky : 0;
+    int kx = ix - a.Nx / 2;
+    kx += kx < 0 ? a.Kx : 0;
+    float val = s22 * sy[iy] * sx[ix] * gp[(size_t)kx * a.Ky + ky].x + g1[(size_t)plane * N + p];
+    if (a.nuclear) {
+      float acc = 0.f;
+      for (int i = 0; i < 2; ++i) {
+        const int qy = a.cover_y[2 * iy + i];
+        if (qy < 0) continue;
+        for (int j = 0; j < 2; ++j) {
+          const int qx = a.cover_x[2 * ix + j];
+          if (qx < 0) continue;
+          const NucFacet f = a.facets[qx * a.Qy + qy];
+          const int ny = f.y1 - f.y0;
+          const int ly = iy - f.y0, lx = ix - f.x0;
+          const int64_t P = (int64_t)ny * (f.x1 - f.x0);
+          const float w = a.wy[f.wy_off + ly] * a.wx[f.wx_off + lx];
+          acc = fmaf(w, v0[(int64_t)grp * a.v0_group + f.v0_off + (int64_t)lc * P + (int64_t)lx * ny + ly], acc);
+        }
+      }
+      val = fmaf(a.sigma00, acc, val);
+    }
+    g[(size_t)plane * N + p] = val;
+  }
+}
+
+__global__ void stats_kernel(const double* __restrict__ primal_part, int nparts, int lg, int G,
+                             const double* __restrict__ blk_stats, const int32_t* __restrict__ ch_nblk,
+                             const int32_t* __restrict__ ch_blkoff, const double* __restrict__ blk_eps,
+                             const double* __restrict__ nuc_vals, int Q, const double* __restrict__ l21_part,
+                             int prox_blocks, double* __restrict__ ring, int* __restrict__ counter) {
+  __shared__ int c;
+  if (threadIdx.x == 0) c = *counter;
+  __syncthreads();
+  double* rec = ring + (size_t)(c % kReportRing) * G * kReportFields;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    double rx = 0, nx = 0, r2 = 0, e2 = 0, nu = 0, l21 = 0;
+    for (int l = g * lg; l < (g + 1) * lg; ++l) {
+      for (int k = 0; k < nparts; ++k) {
+        rx += primal_part[((size_t)l * nparts + k) * 2];
+        nx += primal_part[((size_t)l * nparts + k) * 2 + 1];
+      }
+      for (int b = 0; b < ch_nblk[l]; ++b) {
+        r2 += blk_stats[2 * (ch_blkoff[l] + b) + 1];
+        const double e = blk_eps[(size_t)l * kMaxBlocksPerChannel + b];
+        e2 += e * e;
+      }
+    }
+    if (nuc_vals)
+      for (int q = 0; q < Q; ++q) nu += nuc_vals[g * Q + q];
+    for (int k = 0; k < prox_blocks; ++k) l21 += l21_part[(size_t)g * prox_blocks + k];
+    rec[g * kReportFields + 0] = rx;
+    rec[g * kReportFields + 1] = nx;
+    rec[g * kReportFields + 2] = r2;
+    rec[g * kReportFields + 3] = e2;
+    rec[g * kReportFields + 4] = nu;
+    rec[g * kReportFields + 5] = l21;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *counter = c + 1;
+}
+
+__global__ void weights_kernel(const float* __restrict__ norms, int64_t s, const double* __restrict__ ups,
+                               float* __restrict__ w) {
+  const int g = blockIdx.y;
+  const double u = ups[g];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (int64_t)gridDim.x * blockDim.x) {
+    const double d = norms[(size_t)g * s + i];
+    w[(size_t)g * s + i] = (u + d) > 0 ? (float)(u / (u + d)) : 1.f;
+  }
+}
+
+__global__ void weights0_kernel(const double* __restrict__ sigma, int n, const double* __restrict__ ups,
+                                double* __restrict__ w0) {
+  const int id = blockIdx.x;  // g*Q + q
+  const double u = ups[id];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double d = sigma[(size_t)id * n + i];
+    w0[(size_t)id * n + i] = (u + d) > 0 ? u / (u + d) : 1.0;
+  }
+}
+
+__global__ void diff_norm_kernel(const float* __restrict__ a, const float* __restrict__ b, int64_t n,
+                                 double* __restrict__ out) {
+  double d2 = 0, a2 = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double d = (double)a[i] - b[i];
+    d2 += d * d;
+    a2 += (double)a[i] * a[i];
+  }
+  block_sum2(d2, a2);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = d2;
+    out[2 * blockIdx.x + 1] = a2;
+  }
+}
+
+int nblk(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 8); }
+
+}  // namespace
+
+Solver::~Solver() {
+  if (graph) cudaGraphExecDestroy(graph);
+}
+
+static void solver_launch_iteration(Solver* S, cudaStream_t s) {
+  MeasOp* op = S->op;
+  const int L = S->L;
+  primal_pad_kernel<<<dim3(kPrimalBlocks, L), 256, 0, s>>>(S->x.p, S->g.p, S->xhat.p, op->pad.p, op->sy.p, op->sx.p,
+                                                           S->Ny, S->Nx, op->Ky, op->Kx, S->primal_part.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  fft_forward(op, 0, L, s);
+  launch_degrid_dual(op, 0, L, S->v2.p, S->gold.p, S->y.p, s);
+  launch_block_reduce(op, 0, L, s);
+  launch_grid_dual(op, 0, L, S->v2.p, s);
+  fft_inverse(op, 0, L, s);
+  sara_analysis(S->sp, S->xhat.p, S->coef.p, S->apx.p, L, s);
+  sara_l21_prox(S->sp, S->v1.p, S->coef.p, S->xhat.p, S->w1.p, S->beta1.p, S->G, S->lg, S->l21_part.p, s);
+  sara_synthesis(S->sp, S->v1.p, S->g1.p, S->apx.p, L, (float)S->sigma11, s);
+  if (S->nuclear) {
+    nuc_gram(S->np, S->xhat.p, S->v0.p, s);
+    nuc_eig(S->np, S->w0.p, S->beta0.p, S->nuc_vals.p, s);
+    nuc_reconstruct(S->np, S->xhat.p, S->v0.p, s);
+  }
+  AssembleArgs a;
+  a.Ny = S->Ny;
+  a.Nx = S->Nx;
+  a.Ky = op->Ky;
+  a.Kx = op->Kx;
+  a.lg = S->lg;
+  a.Qy = S->nuclear ? S->np.Qy : 1;
+  a.nuclear = S->nuclear ? 1 : 0;
+  a.sigma00 = (float)S->sigma00;
+  a.facets = S->nuclear ? S->np.d_facets.p : nullptr;
+  a.wy = S->nuclear ? S->np.wy.p : nullptr;
+  a.wx = S->nuclear ? S->np.wx.p : nullptr;
+  a.cover_y = S->nuclear ? S->np.cover_y.p : nullptr;
+  a.cover_x = S->nuclear ? S->np.cover_x.p : nullptr;
+  a.v0_group = S->nuclear ? S->np.v0_group : 0;
+  assemble_kernel<<<dim3(nblk(S->N), L), 256, 0, s>>>(a, S->g.p, op->gridA.p, S->g1.p, S->v0.p, S->sigma22.p,
+                                                     op->sy.p, op->sx.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  stats_kernel<<<1, 64, 0, s>>>(S->primal_part.p, kPrimalBlocks, S->lg, S->G, op->blk_stats.p, op->ch_nblk.p,
+                                op->ch_blkoff.p, op->blk_eps.p, S->nuclear ? S->nuc_vals.p : nullptr,
+                                S->nuclear ? S->np.Q : 0, S->l21_part.p, S->prox_blocks, S->ring.p,
+                                S->ring_counter.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
+static void solver_capture(Solver* S) {
+  cudaStream_t s = S->op->stream;
+  if (S->graph) {
+    cudaGraphExecDestroy(S->graph);
+    S->graph = nullptr;
+  }
+  const unsigned long long before = g_launches;
+  cudaGraph_t g = nullptr;
+  FHS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  try {
+    solver_launch_iteration(S, s);
+  } catch (...) {
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  FHS_CUDA(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(&S->graph, g, 0);
+  cudaGraphDestroy(g);
+  FHS_CUDA(e);
+  S->launches_per_iter = g_launches - before;
+  g_launches = before;
+}
+
+// weights1 from ||Psit x||_row and weights0 from the facet singular values
+// (fhs_update_weights.m:73-92, sara.m:764-768).
+static void solver_update_weights(Solver* S) {
+  cudaStream_t s = S->op->stream;
+  sara_analysis(S->sp, S->x.p, S->coef.p, S->apx.p, S->L, s);
+  sara_row_norms(S->sp, S->coef.p, S->x.p, S->G, S->lg, S->rownorm.p, s);
+  weights_kernel<<<dim3(nblk(S->sp.s), S->G), 256, 0, s>>>(S->rownorm.p, S->sp.s, S->sig.p, S->w1.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  if (S->nuclear) {
+    nuc_gram(S->np, S->x.p, nullptr, s);
+    nuc_eig(S->np, nullptr, nullptr, nullptr, s);
+    weights0_kernel<<<S->G * S->np.Q, 64, 0, s>>>(S->np.sigma.p, S->lg, S->sig_bar.p, S->w0.p);
+    count_launch();
+    FHS_LAUNCH_CHECK();
+  }
+}
+
+}  // namespace fhs
+
+using namespace fhs;
+
+namespace fhs {
+template <class F>
+fhs_status guarded_solver(F&& f) {
+  try {
+    f();
+    set_last_error("");
+    return FHS_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return FHS_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return FHS_ERR_INVALID_ARG;
+  }
+}
+static Solver* sv(fhs_solver* s) {
+  FHS_CHECK(s != nullptr, FHS_ERR_INVALID_ARG, "null solver handle");
+  return reinterpret_cast<Solver*>(s);
+}
+}  // namespace fhs
+
+extern "C" {
+
+fhs_status fhs_solver_create(fhs_measop* op_, const fhs_solver_config* cfg, fhs_solver** out) {
+  return guarded_solver([&] {
+    FHS_CHECK(op_ && cfg && out, FHS_ERR_INVALID_ARG, "null argument");
+    MeasOp* op = reinterpret_cast<MeasOp*>(op_);
+    FHS_CHECK(op->committed, FHS_ERR_STATE, "operator not committed");
+    FHS_CHECK(cfg->algo >= FHS_ALGO_SARA && cfg->algo <= FHS_ALGO_FHS, FHS_ERR_INVALID_ARG, "bad algo");
+    DeviceGuard dg(op->device);
+    cudaStream_t s = op->stream;
+    auto S = std::make_unique<Solver>();
+    S->op = op;
+    S->algo = cfg->algo;
+    S->nlevel = cfg->nlevel > 0 ? cfg->nlevel : 4;
+    S->L = op->L;
+    S->Ny = op->Ny;
+    S->Nx = op->Nx;
+    S->N = op->Npix();
+    if (S->algo == FHS_ALGO_SARA) {
+      S->G = S->L;
+      S->lg = 1;
+      S->nuclear = false;
+    } else {
+      S->G = cfg->n_groups > 0 ? cfg->n_groups : 1;
+      FHS_CHECK(S->L % S->G == 0, FHS_ERR_INVALID_ARG, "channels must split evenly into groups");
+      S->lg = S->L / S->G;
+      S->nuclear = true;
+    }
+    S->sp = sara_plan(S->Ny, S->Nx, S->nlevel);
+    if (S->nuclear) {
+      int Qy = 1, Qx = 1, oy = 0, ox = 0, win = FHS_WINDOW_NONE;
+      std::vector<int> sy, sx;
+      if (S->algo == FHS_ALGO_FHS) {
+        Qy = std::max(cfg->Qy, 1);
+        Qx = std::max(cfg->Qx, 1);
+        oy = std::max(cfg->overlap_y, 0);
+        ox = std::max(cfg->overlap_x, 0);
+        win = cfg->window;
+      }
+      auto splits = [](const int* given, int Q, int N) {
+        std::vector<int> v(Q + 1);
+        for (int q = 0; q <= Q; ++q)
+          v[q] = given ? given[q] : (int)std::floor((double)q * N / Q + 0.5);  // split_range
+        return v;
+      };
+      sy = splits(S->algo == FHS_ALGO_FHS ? cfg->splits_y : nullptr, Qy, S->Ny);
+      sx = splits(S->algo == FHS_ALGO_FHS ? cfg->splits_x : nullptr, Qx, S->Nx);
+      nuc_plan_init(S->np, S->Ny, S->Nx, Qy, Qx, sy, sx, oy, ox, win, S->G, S->lg, s);
+    }
+    const int64_t L = S->L, N = S->N, sc = S->sp.s;
+    S->x.alloc(L * N);
+    S->g.alloc(L * N);
+    S->xhat.alloc(L * N);
+    S->g1.alloc(L * N);
+    S->coef.alloc(L * sc);
+    S->apx.alloc(L * S->sp.apx_total);
+    S->v1.alloc(L * sc);
+    S->w1.alloc((size_t)S->G * sc);
+    S->rownorm.alloc((size_t)S->G * sc);
+    S->beta1.alloc(S->G);
+    S->sig.alloc(S->G);
+    if (S->nuclear) {
+      S->v0.alloc((size_t)S->G * S->np.v0_group);
+      S->w0.alloc((size_t)S->G * S->np.Q * S->lg);
+      S->beta0.alloc((size_t)S->G * S->np.Q);
+      S->sig_bar.alloc((size_t)S->G * S->np.Q);
+      S->nuc_vals.alloc((size_t)S->G * S->np.Q);
+    }
+    S->y.alloc(std::max<int64_t>(op->Mtot, 1));
+    S->y.zero(s);
+    S->v2.alloc(std::max<int64_t>(op->Mtot, 1));
+    S->gold.alloc(std::max<int64_t>(op->Mtot, 1));
+    S->sigma22.alloc(L);
+    S->primal_part.alloc(L * kPrimalBlocks * 2);
+    S->prox_blocks = nblk(sc);
+    S->l21_part.alloc((size_t)S->G * S->prox_blocks);
+    S->ring.alloc((size_t)kReportRing * S->G * kReportFields);
+    S->ring_counter.alloc(1);
+    FHS_CUDA(cudaStreamSynchronize(s));
+    *out = reinterpret_cast<fhs_solver*>(S.release());
+  });
+}
+
+fhs_status fhs_solver_destroy(fhs_solver* s) {
+  return guarded_solver([&] {
+    Solver* S = reinterpret_cast<Solver*>(s);
+    if (!S) return;
+    DeviceGuard dg(S->op->device);
+    delete S;
+  });
+}
+
+fhs_status fhs_solver_set_data(fhs_solver* s_, const double* y, const double* eps) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(y && eps, FHS_ERR_INVALID_ARG, "null buffer");
+    MeasOp* op = S->op;
+    DeviceGuard dg(op->device);
+    cudaStream_t s = op->stream;
+    if (op->stage.n < (size_t)2 * op->Mtot) op->stage.alloc(2 * std::max<int64_t>(op->Mtot, 1));
+    FHS_CUDA(cudaMemcpyAsync(op->stage.p, y, 2 * op->Mtot * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_vis_gather(op->stage.p, S->y.p, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
+    std::vector<double> e((size_t)op->L * kMaxBlocksPerChannel, 0.0);
+    for (int l = 0; l < op->L; ++l)
+      for (int b = 0; b < op->h_nblk[l]; ++b) {
+        const double v = eps[op->h_blkoff[l] + b];
+        FHS_CHECK(std::isfinite(v) && v >= 0, FHS_ERR_INVALID_ARG, "epsilon must be finite and >= 0");
+        e[(size_t)l * kMaxBlocksPerChannel + b] = v;
+      }
+    op->blk_eps.upload(e.data(), e.size(), s);
+    FHS_CUDA(cudaStreamSynchronize(s));
+    S->data_set = true;
+  });
+}
+
+fhs_status fhs_solver_set_params(fhs_solver* s_, const fhs_solver_params* p) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(p && p->nu2 && p->gamma && p->reweighting_sig, FHS_ERR_INVALID_ARG, "null parameter array");
+    FHS_CHECK(!S->nuclear || (p->gamma0 && p->reweighting_sig_bar), FHS_ERR_INVALID_ARG,
+              "gamma0 and reweighting_sig_bar are required");
+    FHS_CHECK(p->nu0 > 0 && p->nu1 > 0, FHS_ERR_INVALID_ARG, "nu0 and nu1 must be > 0");
+    DeviceGuard dg(S->op->device);
+    cudaStream_t s = S->op->stream;
+    const int G = S->G, Q = S->nuclear ? S->np.Q : 0;
+    S->nu2.assign(p->nu2, p->nu2 + S->L);
+    for (double v : S->nu2) FHS_CHECK(v > 0 && std::isfinite(v), FHS_ERR_INVALID_ARG, "nu2 must be > 0");
+    S->gamma.assign(p->gamma, p->gamma + G);
+    S->rw_sig.assign(p->reweighting_sig, p->reweighting_sig + G);
+    if (S->nuclear) {
+      S->gamma0.assign(p->gamma0, p->gamma0 + (size_t)G * Q);
+      S->rw_sig_bar.assign(p->reweighting_sig_bar, p->reweighting_sig_bar + (size_t)G * Q);
+    }
+    S->rw_alpha = p->reweighting_alpha;
+    S->rw_flag = p->reweighting_flag;
+    S->rw_min = p->reweighting_min_iter;
+    S->rw_max = p->reweighting_max_iter;
+    S->rw_rel_var = p->reweighting_rel_var;
+    S->pdfb_min = p->pdfb_min_iter;
+    S->pdfb_max = p->pdfb_max_iter;
+    S->pdfb_rel_var = p->pdfb_rel_var;
+    S->pdfb_tol = p->pdfb_fidelity_tolerance;
+    S->pdfb_rel_var_low = p->pdfb_rel_var_low;
+    const double sigma0 = 1.0 / p->nu0, sigma1 = 1.0 / p->nu1;
+    // facetHyperSARA.m:582-608 / hyperSARA.m:471-487: tau = 0.99/3;
+    // sara.m:502-505: tau = 0.99/(sigma1 nu1 + sigma2 nu2) = 0.99/2
+    S->tau = S->algo == FHS_ALGO_SARA ? 0.99 / 2.0 : 0.99 / 3.0;
+    S->sigma00 = S->tau * sigma0;
+    S->sigma11 = S->tau * sigma1;
+    std::vector<float> s22(S->L);
+    for (int l = 0; l < S->L; ++l) s22[l] = (float)(S->tau / S->nu2[l]);
+    S->sigma22.upload(s22.data(), S->L, s);
+    std::vector<double> b1(G), ups(G);
+    for (int g = 0; g < G; ++g) {
+      b1[g] = S->gamma[g] / sigma1;
+      ups[g] = S->rw_sig[g] * S->rw_alpha;
+    }
+    S->beta1.upload(b1.data(), G, s);
+    S->sig.upload(ups.data(), G, s);
+    if (S->nuclear) {
+      std::vector<double> b0((size_t)G * Q), ub((size_t)G * Q);
+      for (size_t i = 0; i < b0.size(); ++i) {
+        b0[i] = S->gamma0[i] / sigma0;
+        ub[i] = S->rw_sig_bar[i] * S->rw_alpha;
+      }
+      S->beta0.upload(b0.data(), b0.size(), s);
+      S->sig_bar.upload(ub.data(), ub.size(), s);
+    }
+    FHS_CUDA(cudaStreamSynchronize(s));
+    S->params_set = true;
+  });
+}
+
+fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->params_set && S->data_set, FHS_ERR_STATE, "set data and params before init");
+    MeasOp* op = S->op;
+    DeviceGuard dg(op->device);
+    cudaStream_t s = op->stream;
+    const int64_t n = (int64_t)S->L * S->N;
+    if (xinit) {
+      if (op->stage.n < (size_t)n) op->stage.alloc(n);
+      FHS_CUDA(cudaMemcpyAsync(op->stage.p, xinit, n * sizeof(double), cudaMemcpyHostToDevice, s));
+      launch_d2f(op->stage.p, S->x.p, n, s);
+    } else {
+      S->x.zero(s);
+    }
+    S->g.zero(s);
+    S->v1.zero(s);
+    S->v2.zero(s);
+    S->g1.zero(s);
+    if (S->nuclear) S->v0.zero(s);
+    S->ring_counter.zero(s);
+    // Fx_old: keep G A x_init per visibility (linearity of G)
+    launch_pad(op, S->x.p, 0, S->L, s);
+    fft_forward(op, 0, S->L, s);
+    launch_degrid_plain(op, 0, S->L, S->gold.p, s);
+    solver_update_weights(S);
+    FHS_CUDA(cudaStreamSynchronize(s));
+    solver_capture(S);
+    S->iter_done = 0;
+    S->ring_read = 0;
+    S->initialised = true;
+  });
+}
+
+static void read_ring(Solver* S, long long first, int n, std::vector<double>& rec) {
+  cudaStream_t s = S->op->stream;
+  const size_t per = (size_t)S->G * kReportFields;
+  rec.resize((size_t)n * per);
+  for (int i = 0; i < n; ++i) {
+    const long long slot = (first + i) % kReportRing;
+    FHS_CUDA(cudaMemcpyAsync(rec.data() + i * per, S->ring.p + slot * per, per * sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+  }
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+static void fill_info(const Solver* S, const double* rec, fhs_iter_info* info) {
+  double rx = 0, nx = 0, r2 = 0, e2 = 0, nu = 0;
+  for (int g = 0; g < S->G; ++g) {
+    rx += rec[g * kReportFields + 0];
+    nx += rec[g * kReportFields + 1];
+    r2 += rec[g * kReportFields + 2];
+    e2 += rec[g * kReportFields + 3];
+    nu += rec[g * kReportFields + 4];
+  }
+  info->rel_val = nx > 0 ? std::sqrt(rx / nx) : 0.0;
+  info->residual = std::sqrt(r2);
+  info->epsilon = std::sqrt(e2);
+  info->nuclear = nu;
+}
+
+fhs_status fhs_solver_iterate(fhs_solver* s_, int n, fhs_iter_info* info) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+    FHS_CHECK(n >= 0, FHS_ERR_INVALID_ARG, "negative iteration count");
+    DeviceGuard dg(S->op->device);
+    cudaStream_t s = S->op->stream;
+    int done = 0;
+    std::vector<double> rec;
+    while (done < n) {
+      const int chunk = std::min(n - done, kReportRing);
+      for (int i = 0; i < chunk; ++i) FHS_CUDA(cudaGraphLaunch(S->graph, s));
+      g_launches += S->launches_per_iter * chunk;
+      if (info) {
+        read_ring(S, S->iter_done, chunk, rec);
+        for (int i = 0; i < chunk; ++i) fill_info(S, rec.data() + (size_t)i * S->G * kReportFields, info + done + i);
+      }
+      S->iter_done += chunk;
+      done += chunk;
+    }
+    if (!info) FHS_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+fhs_status fhs_solver_update_weights(fhs_solver* s_) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+    DeviceGuard dg(S->op->device);
+    solver_update_weights(S);
+    FHS_CUDA(cudaStreamSynchronize(S->op->stream));
+  });
+}
+
+fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+    DeviceGuard dg(S->op->device);
+    cudaStream_t s = S->op->stream;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (max_iter <= 0) max_iter = (S->rw_max + 1) * S->pdfb_max;
+    const int64_t n = (int64_t)S->L * S->N;
+    DevBuf<float> x_rw;
+    x_rw.alloc(n);
+    FHS_CUDA(cudaMemcpyAsync(x_rw.p, S->x.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    DevBuf<double> dn;
+    const int nb = nblk(n);
+    dn.alloc(2 * nb);
+    std::vector<double> hdn(2 * nb), rec;
+    int last = 0, rw_count = 0, t = 0, converged = 0;
+    fhs_iter_info info{};
+    for (t = 1; t <= max_iter; ++t) {
+      FHS_CUDA(cudaGraphLaunch(S->graph, s));
+      g_launches += S->launches_per_iter;
+      read_ring(S, S->iter_done, 1, rec);
+      S->iter_done += 1;
+      fill_info(S, rec.data(), &info);
+      FHS_CHECK(std::isfinite(info.rel_val) && std::isfinite(info.residual), FHS_ERR_NUMERIC,
+                "non-finite iterate at iteration " + std::to_string(t));
+      const bool pdfb = (t - last >= S->pdfb_min) &&
+                        (t - last >= S->pdfb_max ||
+                         (info.rel_val <= S->pdfb_rel_var && info.residual <= S->pdfb_tol * info.epsilon) ||
+                         info.rel_val <= S->pdfb_rel_var_low);
+      if (!pdfb) continue;
+      diff_norm_kernel<<<nb, 256, 0, s>>>(x_rw.p, S->x.p, n, dn.p);
+      count_launch();
+      FHS_LAUNCH_CHECK();
+      dn.download(hdn.data(), 2 * nb, s);
+      FHS_CUDA(cudaStreamSynchronize(s));
+      double d2 = 0, a2 = 0;
+      for (int i = 0; i < nb; ++i) {
+        d2 += hdn[2 * i];
+        a2 += hdn[2 * i + 1];
+      }
+      const double rel_rw = std::sqrt(d2 / std::max(a2, 1e-300));
+      if (!S->rw_flag || (rw_count >= S->rw_min && (rw_count >= S->rw_max || rel_rw <= S->rw_rel_var))) {
+        converged = 1;
+        break;
+      }
+      solver_update_weights(S);
+      FHS_CUDA(cudaMemcpyAsync(x_rw.p, S->x.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+      ++rw_count;
+      last = t;
+    }
+    FHS_CUDA(cudaStreamSynchronize(s));
+    if (out) {
+      out->n_iter = std::min(t, max_iter);
+      out->n_reweights = rw_count;
+      out->converged = converged;
+      out->rel_val = info.rel_val;
+      out->residual = info.residual;
+      out->epsilon = info.epsilon;
+      out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+  });
+}
+
+fhs_status fhs_solver_get_x(fhs_solver* s_, double* x) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(x != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    MeasOp* op = S->op;
+    DeviceGuard dg(op->device);
+    cudaStream_t s = op->stream;
+    const int64_t n = (int64_t)S->L * S->N;
+    if (op->stage.n < (size_t)n) op->stage.alloc(n);
+    launch_f2d(S->x.p, op->stage.p, n, s);
+    FHS_CUDA(cudaMemcpyAsync(x, op->stage.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FHS_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,49 @@
+// Primal-dual solver state and iteration (see solver.cu).
+#pragma once
+
+#include "measop.cuh"
+#include "nuclear.cuh"
+#include "sara.cuh"
+
+namespace fhs {
+
+constexpr int kReportFields = 6;   // rel_x, norm_x, res^2, eps^2, nuclear, l21 (per group)
+constexpr int kReportRing = 1024;  // iterations kept on the device between host reads
+
+struct Solver {
+  MeasOp* op = nullptr;
+  int algo = FHS_ALGO_FHS, nlevel = 4, G = 1, lg = 1, L = 1, Ny = 0, Nx = 0;
+  int64_t N = 0;
+  SaraPlan sp;
+  NucPlan np;
+  bool nuclear = true;
+
+  DevBuf<float> x, g, xhat, g1, coef, apx, v1, w1, v0, rownorm;
+  DevBuf<double> beta1, w0, beta0, sig_bar, sig;
+  DevBuf<float2> y, v2, gold;
+  DevBuf<float> sigma22;
+  DevBuf<double> primal_part;   // [L][kPrimalBlocks][2]
+  DevBuf<double> l21_part;      // [G][prox blocks]
+  DevBuf<double> nuc_vals;      // [G][Q]
+  DevBuf<double> ring;          // [kReportRing][G][kReportFields]
+  DevBuf<int> ring_counter;
+  int prox_blocks = 0;
+
+  // parameters (host)
+  double tau = 0, sigma00 = 0, sigma11 = 0;
+  std::vector<double> nu2, gamma, gamma0, rw_sig, rw_sig_bar;
+  double rw_alpha = 1.0;
+  int rw_flag = 1, rw_min = 1, rw_max = 20;
+  double rw_rel_var = 1e-4;
+  int pdfb_min = 10, pdfb_max = 2000;
+  double pdfb_rel_var = 5e-5, pdfb_tol = 1.01, pdfb_rel_var_low = 5e-6;
+  bool params_set = false, data_set = false, initialised = false;
+
+  cudaGraphExec_t graph = nullptr;
+  unsigned long long launches_per_iter = 0;
+  long long iter_done = 0;       // iterations since init
+  long long ring_read = 0;       // iterations already read back
+  ~Solver();
+};
+
+}  // namespace fhs

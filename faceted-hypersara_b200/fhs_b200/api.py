@@ -162,3 +162,255 @@ def HS_adjoint_operator_G(y, op: MeasurementOperator):
     x = np.empty(op.Ny * op.Nx * op.L)
     check(lib().fhs_adjoint_operator(op.handle, dptr(flat), dptr(x)))
     return x.reshape(op.Ny, op.Nx, op.L, order="F")
+
+
+def proj_l2ball(x, eps, y, device: int = 0):
+    """src/proj_l2ball.m:20-22 on the GPU (FP64)."""
+    x = np.asarray(x)
+    cplx = np.iscomplexobj(x) or np.iscomplexobj(y)
+    xa = _cplx_in(np.asarray(x, dtype=np.complex128).ravel())
+    ya = _cplx_in(np.asarray(y, dtype=np.complex128).ravel())
+    p = np.empty(x.size, dtype=np.complex128)
+    check(lib().fhs_proj_l2ball(device, x.size, dptr(xa), float(eps), dptr(ya), dptr(p.view(np.float64))))
+    p = p.reshape(x.shape)
+    return p if cplx else p.real.copy()
+
+
+def nuclear_norm(x, device: int = 0):
+    """src/nuclear_norm.m:25-26: x [Ny, Nx, L] (or [N, L])."""
+    x = np.asarray(x, dtype=np.float64)
+    L = x.shape[-1]
+    xm = np.asfortranarray(x.reshape(-1, L, order="F"))
+    f = np.zeros(1)
+    check(lib().fhs_nuclear_norm(device, xm.shape[0], L, dptr(xm.reshape(-1, order="F")), dptr(f)))
+    return float(f[0])
+
+
+def sara_n_coefs(Ny, Nx, nlevel=4):
+    return int(lib().fhs_sara_n_coefs(Ny, Nx, nlevel))
+
+
+def sara_analysis(x, nlevel=4, device: int = 0):
+    """SARA Psit (op_p_sp_wlt_basis): x [Ny, Nx, L] -> coefficients [s, L]."""
+    x = np.asarray(x, dtype=np.float64)
+    if x.ndim == 2:
+        x = x[:, :, None]
+    Ny, Nx, L = x.shape
+    s = sara_n_coefs(Ny, Nx, nlevel)
+    xf = np.asfortranarray(x)
+    out = np.empty((s, L), order="F")
+    check(lib().fhs_sara_analysis(device, Ny, Nx, L, nlevel, dptr(xf.reshape(-1, order="F")),
+                                  dptr(out.reshape(-1, order="F"))))
+    return out
+
+
+def sara_synthesis(c, Ny, Nx, nlevel=4, device: int = 0):
+    """SARA Psi: coefficients [s, L] -> [Ny, Nx, L]."""
+    c = np.asarray(c, dtype=np.float64)
+    if c.ndim == 1:
+        c = c[:, None]
+    L = c.shape[1]
+    cf = np.asfortranarray(c)
+    out = np.empty((Ny, Nx, L), order="F")
+    check(lib().fhs_sara_synthesis(device, Ny, Nx, L, nlevel, dptr(cf.reshape(-1, order="F")),
+                                   dptr(out.reshape(-1, order="F"))))
+    return out
+
+
+def compute_sara_prior(x, nlevel=4, device: int = 0):
+    """src/compute_sara_prior.m:35-41: ||Psit X||_{2,1}."""
+    x = np.asarray(x, dtype=np.float64)
+    if x.ndim == 2:
+        x = x[:, :, None]
+    Ny, Nx, L = x.shape
+    xf = np.asfortranarray(x)
+    f = np.zeros(1)
+    check(lib().fhs_compute_sara_prior(device, Ny, Nx, L, nlevel, dptr(xf.reshape(-1, order="F")), dptr(f)))
+    return float(f[0])
+
+
+def update_dual_data_fidelity(v2, y, x, Fx_old, op: MeasurementOperator, epsilon, sigma22):
+    """src/update_dual_data_fidelity.m:1-6 with pU = 1 and no DR.
+
+    Returns (v2, Ftx, Fx_old, norm_res, global_norm_res, norm_epsilon) with the
+    reference's meaning (v2/norm_res as nested lists, Fx_old [No, L])."""
+    xc = _cube_in(x, op.Ny, op.Nx)
+    v2f = _cplx_in(np.concatenate([op.flatten(v) for v in v2])).copy()
+    yf = _cplx_in(np.concatenate([op.flatten(v) for v in y]))
+    Fo = np.asfortranarray(np.asarray(Fx_old, dtype=np.complex128).reshape(op.No, op.L, order="F"))
+    Fo_flat = np.ascontiguousarray(Fo.T).view(np.float64).copy()   # channel after channel
+    eps = np.concatenate([np.asarray(e, dtype=np.float64).ravel() for e in epsilon])
+    s22 = _f64(np.broadcast_to(np.asarray(sigma22, dtype=np.float64), (op.L,)))
+    Ftx = np.empty(op.Ny * op.Nx * op.L)
+    nres = np.empty(eps.size)
+    gres = np.zeros(1)
+    neps = np.zeros(1)
+    check(lib().fhs_update_dual_data_fidelity(op.handle, dptr(v2f), dptr(yf), dptr(xc.reshape(-1, order="F")),
+                                              dptr(Fo_flat), dptr(eps), dptr(s22), dptr(Ftx), dptr(nres),
+                                              dptr(gres), dptr(neps)))
+    v2c = v2f.view(np.complex128)
+    v2_out, nr_out, pos, bpos = [], [], 0, 0
+    for l in range(op.L):
+        v2_out.append(op.split(l, v2c[pos:pos + op.n_vis[l]]))
+        nb = len(op.block_sizes[l])
+        nr_out.append(list(nres[bpos:bpos + nb]))
+        pos += op.n_vis[l]
+        bpos += nb
+    Fx_new = Fo_flat.view(np.complex128).reshape(op.L, op.No).T.copy(order="F")
+    return (v2_out, Ftx.reshape(op.Ny, op.Nx, op.L, order="F"), Fx_new, nr_out, float(gres[0]),
+            float(neps[0]))
+
+
+# ------------------------------------------------------------------- solvers
+_PARAM_DEFAULTS = dict(
+    nu0=1.0, nu1=1.0, reweighting_alpha=1.0, reweighting_flag=True, reweighting_min_iter=1,
+    reweighting_max_iter=20, reweighting_rel_var=1e-4, pdfb_min_iter=10, pdfb_max_iter=2000,
+    pdfb_rel_var=5e-5, pdfb_fidelity_tolerance=1.01, pdfb_rel_var_low=5e-6)
+
+
+class Solver:
+    """One primal-dual solver on the GPU (facetHyperSARA / hyperSARA / sara).
+
+    ``param``: dict with the reference's ``param`` fields (imaging/imaging.m:839-860):
+    nu2 [L], gamma (per group), gamma0 (per group x facet), reweighting_sig,
+    reweighting_sig_bar, reweighting_*, pdfb_*.
+    """
+
+    def __init__(self, op: MeasurementOperator, algo: int, param: dict, nlevel=4, n_groups=1, Qy=1, Qx=1,
+                 overlap=(0, 0), window="triangular", splits_y=None, splits_x=None):
+        self.op = op
+        self.algo = algo
+        cfg = LB.SolverConfig()
+        cfg.algo = algo
+        cfg.nlevel = nlevel
+        cfg.n_groups = n_groups
+        cfg.Qy, cfg.Qx = Qy, Qx
+        self._sy = None if splits_y is None else (C.c_int * (Qy + 1))(*[int(v) for v in splits_y])
+        self._sx = None if splits_x is None else (C.c_int * (Qx + 1))(*[int(v) for v in splits_x])
+        cfg.splits_y = C.cast(self._sy, C.POINTER(C.c_int)) if self._sy is not None else None
+        cfg.splits_x = C.cast(self._sx, C.POINTER(C.c_int)) if self._sx is not None else None
+        cfg.overlap_y, cfg.overlap_x = int(overlap[0]), int(overlap[1])
+        cfg.window = LB.WINDOW_TRIANGULAR if window == "triangular" else LB.WINDOW_NONE
+        h = C.c_void_p()
+        check(lib().fhs_solver_create(op.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.G = op.L if algo == LB.ALGO_SARA else n_groups
+        self.Q = 0 if algo == LB.ALGO_SARA else (Qy * Qx if algo == LB.ALGO_FHS else 1)
+        self.set_params(param)
+
+    def set_params(self, param: dict):
+        p = dict(_PARAM_DEFAULTS)
+        p.update(param)
+        self._arrays = {}
+
+        def arr(key, n):
+            a = _f64(np.broadcast_to(np.asarray(p[key], dtype=np.float64).ravel(), (n,)) if np.size(p[key]) == 1
+                     else np.asarray(p[key], dtype=np.float64).ravel())
+            if a.size != n:
+                raise ValueError(f"param {key}: expected {n} values, got {a.size}")
+            self._arrays[key] = a
+            return dptr(a)
+
+        sp = LB.SolverParams()
+        sp.nu0, sp.nu1 = float(p["nu0"]), float(p["nu1"])
+        sp.nu2 = arr("nu2", self.op.L)
+        sp.gamma = arr("gamma", self.G)
+        sp.reweighting_sig = arr("reweighting_sig", self.G)
+        if self.Q:
+            sp.gamma0 = arr("gamma0", self.G * self.Q)
+            sp.reweighting_sig_bar = arr("reweighting_sig_bar", self.G * self.Q)
+        sp.reweighting_alpha = float(p["reweighting_alpha"])
+        sp.reweighting_flag = int(bool(p["reweighting_flag"]))
+        sp.reweighting_min_iter = int(p["reweighting_min_iter"])
+        sp.reweighting_max_iter = int(p["reweighting_max_iter"])
+        sp.reweighting_rel_var = float(p["reweighting_rel_var"])
+        sp.pdfb_min_iter = int(p["pdfb_min_iter"])
+        sp.pdfb_max_iter = int(p["pdfb_max_iter"])
+        sp.pdfb_rel_var = float(p["pdfb_rel_var"])
+        sp.pdfb_fidelity_tolerance = float(p["pdfb_fidelity_tolerance"])
+        sp.pdfb_rel_var_low = float(p["pdfb_rel_var_low"])
+        check(lib().fhs_solver_set_params(self._h, C.byref(sp)))
+
+    def set_data(self, y, epsilon):
+        yf = _cplx_in(np.concatenate([self.op.flatten(v) for v in y]))
+        eps = _f64(np.concatenate([np.asarray(e, dtype=np.float64).ravel() for e in epsilon]))
+        check(lib().fhs_solver_set_data(self._h, dptr(yf), dptr(eps)))
+
+    def init(self, xinit=None):
+        if xinit is None:
+            check(lib().fhs_solver_init(self._h, None))
+        else:
+            xc = _cube_in(xinit, self.op.Ny, self.op.Nx)
+            check(lib().fhs_solver_init(self._h, dptr(xc.reshape(-1, order="F"))))
+
+    def iterate(self, n, record=True):
+        info = (LB.IterInfo * max(n, 1))() if record else None
+        check(lib().fhs_solver_iterate(self._h, n, info))
+        if not record:
+            return None
+        return [dict(rel_val=i.rel_val, residual=i.residual, epsilon=i.epsilon, nuclear=i.nuclear)
+                for i in list(info)[:n]]
+
+    def run(self, max_iter=0):
+        ri = LB.RunInfo()
+        check(lib().fhs_solver_run(self._h, int(max_iter), C.byref(ri)))
+        return dict(n_iter=ri.n_iter, n_reweights=ri.n_reweights, converged=bool(ri.converged),
+                    rel_val=ri.rel_val, residual=ri.residual, epsilon=ri.epsilon, seconds=ri.seconds)
+
+    def update_weights(self):
+        check(lib().fhs_solver_update_weights(self._h))
+
+    def x(self):
+        out = np.empty(self.op.Ny * self.op.Nx * self.op.L)
+        check(lib().fhs_solver_get_x(self._h, dptr(out)))
+        return out.reshape(self.op.Ny, self.op.Nx, self.op.L, order="F")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fhs_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def facetHyperSARA(y, epsilon, op: MeasurementOperator, param: dict, Qx, Qy, nlevel=4,
+                   window_type="triangular", overlap_size=(0, 0), xinit=None, n_groups=1, splits_y=None,
+                   splits_x=None, max_iter=0):
+    """src/fhs/facetHyperSARA.m:1-6 -> (xsol [Ny, Nx, L], info).  The
+    reference's A, At, G, W are the operator handle; pU = 1; no DR."""
+    s = Solver(op, LB.ALGO_FHS, param, nlevel, n_groups, Qy, Qx, overlap_size, window_type, splits_y, splits_x)
+    try:
+        s.set_data(y, epsilon)
+        s.init(xinit)
+        info = s.run(max_iter)
+        return s.x(), info
+    finally:
+        s.close()
+
+
+def hyperSARA(y, epsilon, op: MeasurementOperator, param: dict, nlevel=4, xinit=None, n_groups=1, max_iter=0):
+    """src/hs/hyperSARA.m:1-3 -> (xsol, info)."""
+    s = Solver(op, LB.ALGO_HS, param, nlevel, n_groups)
+    try:
+        s.set_data(y, epsilon)
+        s.init(xinit)
+        info = s.run(max_iter)
+        return s.x(), info
+    finally:
+        s.close()
+
+
+def sara(y, epsilon, op: MeasurementOperator, param: dict, nlevel=4, xinit=None, max_iter=0):
+    """src/sara/sara.m:1-3 -> (xsol, info); every channel is its own problem."""
+    s = Solver(op, LB.ALGO_SARA, param, nlevel)
+    try:
+        s.set_data(y, epsilon)
+        s.init(xinit)
+        info = s.run(max_iter)
+        return s.x(), info
+    finally:
+        s.close()

@@ -1,0 +1,101 @@
+"""GPU primal-dual solvers vs the FP64 oracle.
+
+* per-iteration parity: the GPU iterate after k iterations (no stopping, no
+  reweighting) within 2e-5 relative of the oracle's for k <= 20;
+* final reconstruction: same stopping rule and reweighting on both, final
+  SNR (against the ground-truth cube) within 0.05 dB of the oracle's.
+"""
+import numpy as np
+import pytest
+
+from fhs_b200 import synth
+from helpers import rel
+from oracle import problem
+from oracle import solvers as so
+from oracle.facets import FacetGeometry
+
+pytestmark = pytest.mark.gpu
+
+ITER_TOL = 2e-5
+SNR_TOL_DB = 0.05
+
+
+def _setup(algo, Ny=64, Nx=64, L=4, seed=3, Q=(2, 2), overlap=(6, 6), splits=((0, 30, 64), (0, 36, 64))):
+    from fhs_b200 import MeasurementOperator
+    M = Ny * Nx // 2 if L > 1 else 2 * Ny * Nx
+    data, x, meta = problem.make_problem(Ny, Nx, L, M, 2 if L > 1 else 1, seed=seed, synth=synth)
+    nu2 = so.operator_norm(data, 200, 1e-10)
+    if algo == "fhs":
+        geom = FacetGeometry(Ny, Nx, Q[0], Q[1], overlap, splits_y=splits[0], splits_x=splits[1])
+    else:
+        geom = FacetGeometry(Ny, Nx, 1, 1, (0, 0), window_type="none")
+    sig, sig_bar, *_ = so.compute_noise_level(Ny, Nx, L, np.ones(L), "fhs" if algo == "fhs" else "hs",
+                                              geom if algo == "fhs" else None, nu2)
+    if algo == "sara":
+        sig = np.sqrt(1.0 / nu2[0])
+    sig_bar = np.atleast_1d(sig_bar) * np.ones(geom.Q)
+    op = MeasurementOperator(Ny, Nx, meta["om"], meta["blocks"],
+                             [np.full(len(o[0]), 1.0 / s) for o, s in zip(meta["om"], meta["sigma"])])
+    return data, x, op, geom, nu2, sig, sig_bar
+
+
+def _params(nu2, sig, sig_bar, **kw):
+    p = dict(nu2=nu2, gamma=sig, gamma0=sig_bar, reweighting_sig=sig, reweighting_sig_bar=sig_bar)
+    p.update(kw)
+    return p
+
+
+def _gpu_solver(algo, op, param, geom, data):
+    from fhs_b200 import Solver
+    from fhs_b200._lib import ALGO_FHS, ALGO_HS, ALGO_SARA
+    a = {"fhs": ALGO_FHS, "hs": ALGO_HS, "sara": ALGO_SARA}[algo]
+    kw = {}
+    if algo == "fhs":
+        kw = dict(Qy=geom.Qy, Qx=geom.Qx, overlap=(geom.base_y[1][0] - geom.over_y[1][0],
+                                                   geom.base_x[1][0] - geom.over_x[1][0]),
+                  splits_y=[r[0] for r in geom.base_y] + [geom.Ny],
+                  splits_x=[r[0] for r in geom.base_x] + [geom.Nx])
+    s = Solver(op, a, param, **kw)
+    s.set_data(data.y, data.eps)
+    s.init()
+    return s
+
+
+def _oracle_run(algo, data, param, geom, max_iter=None):
+    p = so.SolverParams(**{k: v for k, v in param.items()})
+    if algo == "fhs":
+        return so.facet_hypersara(data, p, geom, max_iter=max_iter)
+    if algo == "hs":
+        return so.hypersara(data, p, max_iter=max_iter)
+    xs, log = so.sara(data, p, max_iter=max_iter)
+    return xs[None], log
+
+
+@pytest.mark.parametrize("algo", ["fhs", "hs", "sara"])
+def test_iterates_match_oracle(algo):
+    L = 1 if algo == "sara" else 4
+    data, x, op, geom, nu2, sig, sig_bar = _setup(algo, L=L)
+    param = _params(nu2, sig, sig_bar, pdfb_min_iter=10 ** 6, reweighting_flag=False)
+    s = _gpu_solver(algo, op, param, geom, data)
+    done = 0
+    for k in (1, 5, 20):
+        s.iterate(k - done)
+        done = k
+        xo, _ = _oracle_run(algo, data, param, geom, max_iter=k)
+        assert rel(np.moveaxis(s.x(), 2, 0), xo) < ITER_TOL, f"{algo} iteration {k}"
+    s.close()
+
+
+@pytest.mark.parametrize("algo", ["fhs", "hs", "sara"])
+def test_final_snr_matches_oracle(algo):
+    L = 1 if algo == "sara" else 4
+    data, x, op, geom, nu2, sig, sig_bar = _setup(algo, L=L, seed=5)
+    param = _params(nu2, sig, sig_bar, pdfb_min_iter=10, pdfb_max_iter=120, reweighting_max_iter=1)
+    s = _gpu_solver(algo, op, param, geom, data)
+    info = s.run()
+    xg = np.moveaxis(s.x(), 2, 0)
+    s.close()
+    xo, log = _oracle_run(algo, data, param, geom)
+    snr_g, snr_o = so.snr_db(x, xg), so.snr_db(x, xo)
+    assert abs(snr_g - snr_o) < SNR_TOL_DB, (snr_g, snr_o, info, log.n_iter)
+    assert snr_o > 15.0
