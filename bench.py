@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Throughput of the Faceted HyperSARA primal-dual iteration on B200.
+
+Workload (batched Faceted HyperSARA, synthetic): 1024 x 1024 x 64 cube over
+1-2 GHz, C = 4 interleaved spectral sub-cubes of 16 channels, 4 x 4 spatial
+facets (+-15% jitter, 10% overlap, triangular apodisation), per-channel
+visibilities uniform in [0.3 N, 1.0 N] in 2-6 random blocks, 40 dB input SNR.
+One step = one primal-dual iteration of the whole cube (all sub-cubes,
+facets and blocks), replayed as one CUDA graph.  The working set (tens of
+GB) is far larger than the 126 MB L2, so no flush is needed between steps.
+
+`python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]`
+prints one JSON line on rank 0.  Under torchrun every rank solves its own
+cube (independent problems, no data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "faceted-hypersara_b200"))
+
+METRIC = "FHS 1024²×64 iter/s & time-to-converge: warm-start vs plain, 1×B200"
+UNIT = "iter/s"
+WORKLOAD = dict(Ny=1024, Nx=1024, L=64, C=4, Q=4, overlap_frac=0.1, jitter=0.15, m_lo=0.3, m_hi=1.0,
+                blocks=(2, 6), snr_db=40.0)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _config(extra=None):
+    cfg = {"workload": "fhs_1024x1024x64_C4_Q4x4_overlap10pct", "Ny": 1024, "Nx": 1024, "L": 64,
+           "spectral_subcubes": 4, "facets": "4x4 (+-15% jitter), 10% overlap, triangular",
+           "vis_per_channel": "U[0.3N, 1.0N], 2-6 blocks", "nufft": "7x7 min-max KB, 2x oversampling",
+           "sara": "db1-db8 + Dirac, 4 levels", "precision": "f32 data/FFT/DWT/prox, f64 norms/eig/stopping",
+           "l2": "inputs larger than L2 (working set tens of GB), no flush"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, device_index):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-i", str(device_index), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.p is None:
+            return out
+        time.sleep(0.3)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return out
+        sm = sorted(float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit())
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].strip() == "Active":
+                    reasons.add(n)
+        out["sm_mhz"] = sm[len(sm) // 2] if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(rows)
+        return out
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _init_pg(world, local):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def _max_over_ranks(dist, value, local):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist, local):
+    if dist is not None:
+        import torch
+        dist.barrier(device_ids=[local])
+        torch.cuda.synchronize(local)
+
+
+def algorithmic_bytes(prob, sp_s):
+    """Algorithmic HBM bytes per launch of each hand-written stage, whole cube."""
+    op = prob["op"]
+    L, N, M = op.L, op.Ny * op.Nx, prob["n_vis"]
+    No = op.No
+    Q = prob["Q"]
+    sy, sx = prob["splits"]
+    ov = prob["overlap"][0]
+    from fhs_b200.heuristics import facet_pixels
+    P = sum(facet_pixels(sy, sx, (ov, ov)))
+    s_w = sp_s - N
+    return {
+        "primal_pad": N * L * (4 + 4) + N * L * (4 + 4 + 8),
+        "degrid_dual": No * L * 8 + M * (16 + 8 + 8 + 8) + M * (8 + 8),
+        "grid_dual": M * (16 + 8) + M * 8 + No * L * 8,
+        "sara_analysis": N * L * 4 + s_w * L * 4,
+        "l21_prox": 2 * sp_s * L * 4 + s_w * L * 4 + N * L * 4 + sp_s * 4 * prob["C"],
+        "sara_synthesis": sp_s * L * 4 + N * L * 4,
+        "facet_gram": 2 * P * L * 4,
+        "facet_reconstruct": 3 * P * L * 4,
+        "assemble_g": N * L * (8 + 4 + 4) + P * L * 4,
+    }
+
+
+def _traffic_from_profiles(kernel):
+    """dram bytes per launch of `kernel` from a committed ncu summary, if any."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.startswith(kernel) or not f.endswith(".md"):
+            continue
+        with open(os.path.join(d, f)) as fh:
+            for line in fh:
+                if line.strip().startswith("dram_bytes_per_launch_full ="):
+                    try:
+                        return float(line.split("=")[1].split()[0])
+                    except Exception:
+                        return None
+    return None
+
+
+def cpu_sample_seconds(seed=0, n_iter=1):
+    """Oracle (FP64 NumPy/SciPy, all host threads) time of one FHS iteration on
+    one channel of one sub-cube at full resolution (1024 x 1024, all of that
+    channel's visibilities, 4x4 facets); the whole-cube estimate scales it by
+    the 64 channels."""
+    import numpy as np
+
+    from fhs_b200 import synth
+    from oracle import solvers as so
+    from oracle.facets import FacetGeometry
+    from oracle.nufft import NufftOperator
+    rng = np.random.default_rng(seed)
+    Ny = Nx = WORKLOAD["Ny"]
+    N = Ny * Nx
+    M = int(rng.integers(int(0.3 * N), N + 1))
+    x = synth.sky_image(Ny, Nx, seed)[None]
+    om_y, om_x = synth.base_coverage(M, seed)
+    op = NufftOperator(Ny, Nx)
+    G = op.G(om_y, om_x)
+    y = [G @ op.A(x[0])]
+    data = so.DataTerm(op, [[G]], [y], [[float(np.sqrt(M + 2 * np.sqrt(M)))]])
+    geom = FacetGeometry(Ny, Nx, 4, 4, (26, 26))
+    p = so.SolverParams(nu2=np.array([1e3]), gamma=1e-3, gamma0=np.full(16, 1e-2), reweighting_sig=1e-3,
+                        reweighting_sig_bar=np.full(16, 1e-2), pdfb_min_iter=10 ** 6, reweighting_flag=False)
+    so.facet_hypersara(data, p, geom, max_iter=1)   # warm-up (allocations, FFT plans)
+    t0 = time.perf_counter()
+    so.facet_hypersara(data, p, geom, max_iter=n_iter)
+    return (time.perf_counter() - t0) / n_iter
+
+
+def _ncores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    world, rank, local = _dist()
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(_ncores()))
+    L = WORKLOAD["L"]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t = cpu_sample_seconds(seed=i)
+        if i >= args.warmup:
+            times.append(t)
+    per_cube = sum(times) / len(times) * L
+    value = 1.0 / per_cube
+    sample = (f"one FHS iteration of the FP64 oracle on 1 channel (1024x1024, its full visibility set, 4x4 "
+              f"facets), x{L} channels for the whole cube; {args.steps} steps")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_cube * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": _config({"reference": "oracle port (MATLAB reference not runnable here)"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": _ncores(), "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+
+    world, rank, local = _dist()
+    dist = _init_pg(world, local)
+    from fhs_b200 import lib
+    from fhs_b200.workload import build_problem, make_solver
+    seed = 1000 + rank
+    prob = build_problem(**WORKLOAD, seed=seed, device=local)
+    s = make_solver(prob)
+    s.init()
+    s.iterate(args.warmup, record=False)
+    # ---- timed region: K graph replays, CUDA events on the solver stream
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    smi_index = vis.split(",")[local] if vis else str(local)
+    sampler = ClockSampler(smi_index)
+    _barrier(dist, local)
+    l0 = lib().fhs_kernel_launch_count()
+    ms = s.time_iterations(args.steps)
+    launches = lib().fhs_kernel_launch_count() - l0
+    _barrier(dist, local)
+    clocks = sampler.stop()
+    ms_max = _max_over_ranks(dist, ms, local)
+    value = world * args.steps / (ms_max / 1e3)
+    # ---- per-stage device times (same stream, stage-by-stage launches)
+    stages = s.profile_stages(3)
+    from fhs_b200 import sara_n_coefs
+    nbytes = algorithmic_bytes(prob, sara_n_coefs(1024, 1024, 4))
+    mine = {k: v for k, v in stages.items() if k in nbytes}
+    dom = max(mine, key=mine.get)
+    peak, peak_kind = _peaks()
+    achieved = nbytes[dom] / (mine[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                "algorithmic_bytes": nbytes[dom], "ms_per_launch": mine[dom],
+                "traffic": _traffic_from_profiles(dom)}
+    stage_rows = {k: {"ms": round(v, 4), **({"gbs": round(nbytes[k] / (v / 1e3) / 1e9, 1)} if k in nbytes and v > 0
+                                           else {})} for k, v in stages.items()}
+    # ---- end to end through the public API with pinned host buffers
+    e2e = None
+    try:
+        e2e = _e2e(prob, s, args.steps)
+    except Exception as e:  # reported, not hidden
+        e2e = {"error": str(e)}
+    e2e_v = _max_over_ranks(dist, e2e.get("seconds", 0.0), local) if "seconds" in e2e else None
+    if e2e_v:
+        e2e = {"value": world * args.steps / e2e_v, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"],
+               "d2h_bytes_per_step": e2e["d2h"],
+               "what": "per call: fhs_solver_set_data (pinned y) + fhs_solver_init + K iterations + "
+                       "fhs_solver_get_x, host wall clock"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t = cpu_sample_seconds()
+        cpu = {"value": 1.0 / (t * WORKLOAD["L"]), "unit": UNIT, "cores": _ncores(), "kind": "port",
+               "sample": "one FHS iteration of the FP64 oracle on 1 channel at 1024x1024 (its full visibility "
+                         "set, 4x4 facets), scaled by 64 channels"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": _config({"visibilities": prob["n_vis"], "parallelism": f"{world} independent cubes"}),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks, "stages_ms": stage_rows,
+                "vis_per_s": 2.0 * prob["n_vis"] * value}
+        print(json.dumps(line), flush=True)
+    s.close()
+    prob["op"].close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def _e2e(prob, s, steps):
+    """Public-API call with host buffers: y and x in pinned host memory."""
+    import numpy as np
+    import torch
+    op = prob["op"]
+    yflat = np.concatenate([op.flatten(v) for v in prob["y"]])
+    ypin = torch.empty(yflat.size * 2, dtype=torch.float64, pin_memory=True).numpy()
+    ypin[:] = yflat.view(np.float64)
+    eps = np.concatenate([np.asarray(e, dtype=np.float64) for e in prob["eps"]])
+    xpin = torch.empty(op.Ny * op.Nx * op.L, dtype=torch.float64, pin_memory=True).numpy()
+    import ctypes as C
+
+    from fhs_b200._lib import check, dptr, lib
+    t0 = time.perf_counter()
+    check(lib().fhs_solver_set_data(s._h, dptr(ypin), dptr(eps)))
+    check(lib().fhs_solver_init(s._h, None))
+    check(lib().fhs_solver_iterate(s._h, steps, None))
+    check(lib().fhs_solver_get_x(s._h, dptr(xpin)))
+    dt = time.perf_counter() - t0
+    del C
+    return {"seconds": dt, "h2d": int((ypin.nbytes + eps.nbytes) / steps), "d2h": int(xpin.nbytes / steps)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

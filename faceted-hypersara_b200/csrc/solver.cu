@@ -209,26 +209,48 @@ Solver::~Solver() {
   if (graph) cudaGraphExecDestroy(graph);
 }
 
-static void solver_launch_iteration(Solver* S, cudaStream_t s) {
+static const char* kStageNames[] = {"primal_pad", "fft_forward", "degrid_dual", "block_reduce", "grid_dual",
+                                    "fft_inverse", "sara_analysis", "l21_prox", "sara_synthesis", "facet_gram",
+                                    "facet_eig", "facet_reconstruct", "assemble_g", "stats"};
+constexpr int kStages = sizeof(kStageNames) / sizeof(kStageNames[0]);
+
+// Records ev[k] after stage k-1 (ev[0] before the first) when ev is non-null.
+static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev = nullptr) {
   MeasOp* op = S->op;
   const int L = S->L;
+  int stage = 0;
+  auto mark = [&]() {
+    if (ev) FHS_CUDA(cudaEventRecord(ev[stage], s));
+    ++stage;
+  };
+  mark();
   primal_pad_kernel<<<dim3(kPrimalBlocks, L), 256, 0, s>>>(S->x.p, S->g.p, S->xhat.p, op->pad.p, op->sy.p, op->sx.p,
                                                            S->Ny, S->Nx, op->Ky, op->Kx, S->primal_part.p);
   count_launch();
   FHS_LAUNCH_CHECK();
+  mark();
   fft_forward(op, 0, L, s);
+  mark();
   launch_degrid_dual(op, 0, L, S->v2.p, S->gold.p, S->y.p, s);
+  mark();
   launch_block_reduce(op, 0, L, s);
+  mark();
   launch_grid_dual(op, 0, L, S->v2.p, s);
+  mark();
   fft_inverse(op, 0, L, s);
+  mark();
   sara_analysis(S->sp, S->xhat.p, S->coef.p, S->apx.p, L, s);
+  mark();
   sara_l21_prox(S->sp, S->v1.p, S->coef.p, S->xhat.p, S->w1.p, S->beta1.p, S->G, S->lg, S->l21_part.p, s);
+  mark();
   sara_synthesis(S->sp, S->v1.p, S->g1.p, S->apx.p, L, (float)S->sigma11, s);
-  if (S->nuclear) {
-    nuc_gram(S->np, S->xhat.p, S->v0.p, s);
-    nuc_eig(S->np, S->w0.p, S->beta0.p, S->nuc_vals.p, s);
-    nuc_reconstruct(S->np, S->xhat.p, S->v0.p, s);
-  }
+  mark();
+  if (S->nuclear) nuc_gram(S->np, S->xhat.p, S->v0.p, s);
+  mark();
+  if (S->nuclear) nuc_eig(S->np, S->w0.p, S->beta0.p, S->nuc_vals.p, s);
+  mark();
+  if (S->nuclear) nuc_reconstruct(S->np, S->xhat.p, S->v0.p, s);
+  mark();
   AssembleArgs a;
   a.Ny = S->Ny;
   a.Nx = S->Nx;
@@ -248,12 +270,14 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s) {
                                                      op->sy.p, op->sx.p);
   count_launch();
   FHS_LAUNCH_CHECK();
+  mark();
   stats_kernel<<<1, 64, 0, s>>>(S->primal_part.p, kPrimalBlocks, S->lg, S->G, op->blk_stats.p, op->ch_nblk.p,
                                 op->ch_blkoff.p, op->blk_eps.p, S->nuclear ? S->nuc_vals.p : nullptr,
                                 S->nuclear ? S->np.Q : 0, S->l21_part.p, S->prox_blocks, S->ring.p,
                                 S->ring_counter.p);
   count_launch();
   FHS_LAUNCH_CHECK();
+  mark();
 }
 
 static void solver_capture(Solver* S) {
@@ -655,6 +679,60 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
       out->epsilon = info.epsilon;
       out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
+  });
+}
+
+int fhs_solver_stage_count(void) { return kStages; }
+
+const char* fhs_solver_stage_name(int i) { return (i >= 0 && i < kStages) ? kStageNames[i] : ""; }
+
+fhs_status fhs_solver_time_iterations(fhs_solver* s_, int n, double* ms) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+    FHS_CHECK(n > 0 && ms, FHS_ERR_INVALID_ARG, "bad arguments");
+    DeviceGuard dg(S->op->device);
+    cudaStream_t s = S->op->stream;
+    cudaEvent_t e0, e1;
+    FHS_CUDA(cudaEventCreate(&e0));
+    FHS_CUDA(cudaEventCreate(&e1));
+    FHS_CUDA(cudaStreamSynchronize(s));
+    FHS_CUDA(cudaEventRecord(e0, s));
+    for (int i = 0; i < n; ++i) FHS_CUDA(cudaGraphLaunch(S->graph, s));
+    FHS_CUDA(cudaEventRecord(e1, s));
+    FHS_CUDA(cudaEventSynchronize(e1));
+    float t = 0.f;
+    FHS_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g_launches += S->launches_per_iter * n;
+    S->iter_done += n;
+    *ms = t;
+  });
+}
+
+fhs_status fhs_solver_profile_stages(fhs_solver* s_, int n, double* stage_ms) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+    FHS_CHECK(n > 0 && stage_ms, FHS_ERR_INVALID_ARG, "bad arguments");
+    DeviceGuard dg(S->op->device);
+    cudaStream_t s = S->op->stream;
+    cudaEvent_t ev[kStages + 1];
+    for (auto& e : ev) FHS_CUDA(cudaEventCreate(&e));
+    std::vector<double> acc(kStages, 0.0);
+    for (int it = 0; it < n; ++it) {
+      solver_launch_iteration(S, s, ev);
+      FHS_CUDA(cudaEventSynchronize(ev[kStages]));
+      for (int k = 0; k < kStages; ++k) {
+        float t = 0.f;
+        FHS_CUDA(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        acc[k] += t;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    S->iter_done += n;
+    for (int k = 0; k < kStages; ++k) stage_ms[k] = acc[k] / n;
   });
 }
 

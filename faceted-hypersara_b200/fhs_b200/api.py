@@ -360,6 +360,19 @@ class Solver:
     def update_weights(self):
         check(lib().fhs_solver_update_weights(self._h))
 
+    def time_iterations(self, n):
+        """Device milliseconds of n graph replays (CUDA events on the solver stream)."""
+        ms = np.zeros(1)
+        check(lib().fhs_solver_time_iterations(self._h, int(n), dptr(ms)))
+        return float(ms[0])
+
+    def profile_stages(self, n):
+        """Mean device milliseconds per iteration stage over n iterations."""
+        k = int(lib().fhs_solver_stage_count())
+        ms = np.zeros(k)
+        check(lib().fhs_solver_profile_stages(self._h, int(n), dptr(ms)))
+        return {lib().fhs_solver_stage_name(i).decode(): float(ms[i]) for i in range(k)}
+
     def x(self):
         out = np.empty(self.op.Ny * self.op.Nx * self.op.L)
         check(lib().fhs_solver_get_x(self._h, dptr(out)))

@@ -97,3 +97,12 @@ def noise(M: int, rng) -> np.ndarray:
 
 def noise_sigma(y0: np.ndarray, snr_db: float) -> float:
     return float(10.0 ** (-snr_db / 20.0) * np.linalg.norm(y0) / np.sqrt(y0.size))
+
+
+def jittered_splits(nchunks: int, N: int, jitter: float, rng) -> list:
+    """Facet boundaries 0..N with sizes uniform in (1 +- jitter) x N/nchunks."""
+    w = rng.uniform(1.0 - jitter, 1.0 + jitter, size=nchunks)
+    edges = np.concatenate([[0.0], np.cumsum(w) / np.sum(w) * N])
+    s = np.floor(edges + 0.5).astype(int)
+    s[0], s[-1] = 0, N
+    return [int(v) for v in s]

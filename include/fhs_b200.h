@@ -206,6 +206,16 @@ FHS_API fhs_status fhs_solver_get_x(fhs_solver* s, double* x);
 /* Recompute reweighting weights from the current x (fhs_update_weights.m). */
 FHS_API fhs_status fhs_solver_update_weights(fhs_solver* s);
 
+/* Measurement hooks (no reference counterpart: the reference times its
+ * phases with tic/toc, src/fhs/facetHyperSARA.m:703-716,771-776).
+ * time_iterations: n graph replays bracketed by CUDA events on the solver's
+ * stream, total device milliseconds.  profile_stages: n iterations launched
+ * stage by stage with events in between, mean milliseconds per stage. */
+FHS_API int fhs_solver_stage_count(void);
+FHS_API const char* fhs_solver_stage_name(int i);
+FHS_API fhs_status fhs_solver_time_iterations(fhs_solver* s, int n, double* ms);
+FHS_API fhs_status fhs_solver_profile_stages(fhs_solver* s, int n, double* stage_ms);
+
 #ifdef __cplusplus
 }
 #endif

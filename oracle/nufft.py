@@ -37,6 +37,7 @@ Conventions (parity against the MATLAB submodule is unpinned):
 from __future__ import annotations
 
 import numpy as np
+import scipy.fft as sfft
 import scipy.sparse as sp
 from scipy.special import i0
 
@@ -188,13 +189,13 @@ class NufftOperator:
 
     def A(self, x):
         """x [Ny, Nx] real -> Fx (No,) complex, column-major vectorisation."""
-        Y = np.fft.fft2(self.scale * x, s=(self.Ky, self.Kx))
+        Y = sfft.fft2(self.scale * x, s=(self.Ky, self.Kx), workers=-1)
         return Y.reshape(-1, order="F")
 
     def At(self, Fx):
         """Fx (No,) complex -> [Ny, Nx] complex (exact adjoint of A)."""
         Y = np.asarray(Fx).reshape(self.Ky, self.Kx, order="F")
-        x = np.fft.ifft2(Y) * self.No
+        x = sfft.ifft2(Y, workers=-1) * self.No
         return self.scale * x[: self.Ny, : self.Nx]
 
     def G(self, om_y, om_x, weights=None):
