@@ -30,6 +30,8 @@ METRIC = "FHS 1024²×64 iter/s & time-to-converge: warm-start vs plain, 1×B200
 UNIT = "iter/s"
 WORKLOAD = dict(Ny=1024, Nx=1024, L=64, C=4, Q=4, overlap_frac=0.1, jitter=0.15, m_lo=0.3, m_hi=1.0,
                 blocks=(2, 6), snr_db=40.0)
+# reduced case for ncu captures (same kernels, ~0.6 GB of grids)
+SMALL = dict(WORKLOAD, Ny=512, Nx=512, L=16)
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -247,7 +249,8 @@ def run_ours(args):
     from fhs_b200 import lib
     from fhs_b200.workload import build_problem, make_solver
     seed = 1000 + rank
-    prob = build_problem(**WORKLOAD, seed=seed, device=local)
+    wl = SMALL if args.case == "small" else WORKLOAD
+    prob = build_problem(**wl, seed=seed, device=local)
     s = make_solver(prob)
     s.init()
     s.iterate(args.warmup, record=False)
@@ -266,7 +269,7 @@ def run_ours(args):
     # ---- per-stage device times (same stream, stage-by-stage launches)
     stages = s.profile_stages(3)
     from fhs_b200 import sara_n_coefs
-    nbytes = algorithmic_bytes(prob, sara_n_coefs(1024, 1024, 4))
+    nbytes = algorithmic_bytes(prob, sara_n_coefs(wl["Ny"], wl["Nx"], 4))
     mine = {k: v for k, v in stages.items() if k in nbytes}
     dom = max(mine, key=mine.get)
     peak, peak_kind = _peaks()
@@ -290,7 +293,7 @@ def run_ours(args):
                "what": "per call: fhs_solver_set_data (pinned y) + fhs_solver_init + K iterations + "
                        "fhs_solver_get_x, host wall clock"}
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.case == "full":
         t = cpu_sample_seconds()
         cpu = {"value": 1.0 / (t * WORKLOAD["L"]), "unit": UNIT, "cores": _ncores(), "kind": "port",
                "sample": "one FHS iteration of the FP64 oracle on 1 channel at 1024x1024 (its full visibility "
@@ -299,7 +302,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": _config({"visibilities": prob["n_vis"], "parallelism": f"{world} independent cubes"}),
+                "config": _config({"visibilities": prob["n_vis"], "parallelism": f"{world} independent cubes"})
+                if args.case == "full" else {"workload": "fhs_512x512x16_C4_Q4x4 (profiling case)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks, "stages_ms": stage_rows,
                 "vis_per_s": 2.0 * prob["n_vis"] * value}
@@ -341,6 +345,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["full", "small"], default="full",
+                    help="small: 512x512x16 profiling case for ncu captures (not a bench line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

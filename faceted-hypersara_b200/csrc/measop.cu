@@ -11,8 +11,8 @@
 //   f32 weight), y / v2 / GFx_old c64.
 // The image is placed at (n - N/2) mod K before the FFT, which moves the
 // reference's centring phase exp(i om N/2) out of G: every tap coefficient is
-// then a function of the fractional grid offset only and is read from a
-// 1024-sample table (linear interpolation, < 2e-7 relative error).
+// then a function of the fractional grid offset only, evaluated from degree-8
+// polynomials fitted (FP64, host) to the exact min-max coefficients.
 //
 // The l2-ball dual takes two passes because the block norm ||z_b|| is a
 // reduction over all of a block's visibilities: pass 1 writes z to a scratch
@@ -38,7 +38,7 @@ unsigned long long g_launches = 0;
 namespace {
 
 constexpr int kS = kTableSamples;
-constexpr int kSmemPitch = kTileCells + kMaxTaps - 1;  // 71
+constexpr int kSmemPitch = kTileCells + kBinCells;  // 72 (>= 64 + J - 1)
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -50,17 +50,20 @@ __device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {  // a*b +
   return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
 }
 
+// Tap coefficients h_j(f) of one axis by Horner evaluation of degree-8
+// polynomials in f - 1/2 (FP32, < 1e-7 relative to the FP64 construction).
 template <int J>
-__device__ __forceinline__ void taps(const float2* __restrict__ tab, float f, float2 (&h)[J]) {
-  const float u = f * (float)kS;
-  int iu = (int)u;
-  iu = iu < 0 ? 0 : (iu > kS - 1 ? kS - 1 : iu);
-  const float t = u - (float)iu;
+__device__ __forceinline__ void taps(const float (&P)[kMaxTaps][2][kPolyDegree + 1], float f, float2 (&h)[J]) {
+  const float s = f - 0.5f;
 #pragma unroll
   for (int j = 0; j < J; ++j) {
-    const float2 a = __ldg(tab + j * (kS + 1) + iu);
-    const float2 b = __ldg(tab + j * (kS + 1) + iu + 1);
-    h[j] = make_float2(fmaf(t, b.x - a.x, a.x), fmaf(t, b.y - a.y, a.y));
+    float re = P[j][0][kPolyDegree], im = P[j][1][kPolyDegree];
+#pragma unroll
+    for (int k = kPolyDegree - 1; k >= 0; --k) {
+      re = fmaf(re, s, P[j][0][k]);
+      im = fmaf(im, s, P[j][1][k]);
+    }
+    h[j] = make_float2(re, im);
   }
 }
 
@@ -76,9 +79,11 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
                                                      float2* __restrict__ gold,
                                                      const float2* __restrict__ y,
                                                      double* __restrict__ partials, float2* __restrict__ zbuf) {
-  __shared__ float2 sm[(kTileCells + J - 1) * (kTileCells + J - 1)];
+  // pitch 72 along y: starts within a sub-bin spread over distinct bank pairs
+  constexpr int P = kSmemPitch;
+  constexpr int R = kTileCells + J - 1;
+  __shared__ float2 sm[R * P];
   __shared__ double bacc[kMaxBlocksPerChannel * 2];
-  constexpr int P = kTileCells + J - 1;
   const int tile = blockIdx.x;
   const int ch = c0 + blockIdx.y;
   const int t0 = tile % op.nT0, t1 = tile / op.nT0;
@@ -95,10 +100,10 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
   }
   const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
   const float2* g = grid + (size_t)ch * op.Ky * op.Kx;
-  for (int idx = threadIdx.x; idx < P * P; idx += blockDim.x) {
-    const int c1 = idx / P, cc0 = idx - c1 * P;
+  for (int idx = threadIdx.x; idx < R * R; idx += blockDim.x) {
+    const int c1 = idx / R, cc0 = idx - c1 * R;
     const int k0 = wrap(a0 + cc0, op.Ky), k1 = wrap(a1 + c1, op.Kx);
-    sm[idx] = __ldg(g + (size_t)k1 * op.Ky + k0);
+    sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * op.Ky + k0);
   }
   __syncthreads();
   const int64_t vo = op.ch_voff[ch];
@@ -108,8 +113,8 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
     const int d0 = (int)(kp & 0x3FFFu) - a0;
     const int d1 = (int)((kp >> 14) & 0x3FFFu) - a1;
     float2 hy[J], hx[J];
-    taps<J>(op.tab_y, gm.x, hy);
-    taps<J>(op.tab_x, gm.y, hx);
+    taps<J>(op.py, gm.x, hy);
+    taps<J>(op.px, gm.y, hx);
     float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
     for (int jx = 0; jx < J; ++jx) {
@@ -160,8 +165,8 @@ __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict
                                                    float2* __restrict__ v2,
                                                    const float* __restrict__ blk_scale,
                                                    const float2* __restrict__ zbuf) {
-  __shared__ float acc_re[kTileCells * kTileCells];
-  __shared__ float acc_im[kTileCells * kTileCells];
+  __shared__ float acc_re[kTileCells * kSmemPitch];
+  __shared__ float acc_im[kTileCells * kSmemPitch];
   __shared__ Range rng[2 + 2 * kSubPerTile];
   __shared__ int nrng;
   __shared__ int total;
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict
   const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
   const int T0 = min(kTileCells, op.Ky - a0), T1 = min(kTileCells, op.Kx - a1);
   const int32_t* off = op.sb_off + (size_t)ch * (op.nkeys + 1);
-  for (int i = threadIdx.x; i < kTileCells * kTileCells; i += blockDim.x) {
+  for (int i = threadIdx.x; i < kTileCells * kSmemPitch; i += blockDim.x) {
     acc_re[i] = 0.f;
     acc_im[i] = 0.f;
   }
@@ -229,8 +234,8 @@ __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict
     }
     if (d0 + J <= 0 || d0 >= T0 || d1 + J <= 0 || d1 >= T1) continue;
     float2 hy[J], hx[J];
-    taps<J>(op.tab_y, gm.x, hy);
-    taps<J>(op.tab_x, gm.y, hx);
+    taps<J>(op.py, gm.x, hy);
+    taps<J>(op.px, gm.y, hx);
     v.x *= gm.w;
     v.y *= gm.w;
 #pragma unroll
@@ -243,8 +248,8 @@ __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict
         const int cc0 = d0 + jy;
         if ((unsigned)cc0 >= (unsigned)T0) continue;
         const float2 a = cmulc(hy[jy], t);
-        atomicAdd(&acc_re[c1 * kTileCells + cc0], a.x);
-        atomicAdd(&acc_im[c1 * kTileCells + cc0], a.y);
+        atomicAdd(&acc_re[c1 * kSmemPitch + cc0], a.x);
+        atomicAdd(&acc_im[c1 * kSmemPitch + cc0], a.y);
       }
     }
   }
@@ -253,7 +258,7 @@ __global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict
   for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
     const int c1 = idx / T0, cc0 = idx - c1 * T0;
     gb[(size_t)(a1 + c1) * op.Ky + a0 + cc0] =
-        make_float2(acc_re[c1 * kTileCells + cc0], acc_im[c1 * kTileCells + cc0]);
+        make_float2(acc_re[c1 * kSmemPitch + cc0], acc_im[c1 * kSmemPitch + cc0]);
   }
 }
 
@@ -337,6 +342,13 @@ int grid_blocks(int64_t n, int threads) {
 // ------------------------------------------------------------- host side
 OpView MeasOp::view() const {
   OpView v;
+  const int nt = kPolyDegree + 1;
+  for (int j = 0; j < kMaxTaps; ++j)
+    for (int part = 0; part < 2; ++part)
+      for (int k = 0; k < nt; ++k) {
+        v.py[j][part][k] = j < Jy ? (float)ay.poly[((size_t)j * 2 + part) * nt + k] : 0.f;
+        v.px[j][part][k] = j < Jx ? (float)ax.poly[((size_t)j * 2 + part) * nt + k] : 0.f;
+      }
   v.Ny = Ny;
   v.Nx = Nx;
   v.Ky = Ky;

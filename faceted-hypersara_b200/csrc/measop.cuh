@@ -8,6 +8,9 @@ namespace fhs {
 
 // Read-only view of the operator passed to kernels by value.
 struct OpView {
+  // tap polynomials (kernel parameters: uniform across threads)
+  float py[kMaxTaps][2][kPolyDegree + 1];
+  float px[kMaxTaps][2][kPolyDegree + 1];
   int Ny, Nx, Ky, Kx, Jy, Jx;
   int nT0, nT1;      // tiles per axis (kTileCells cells each, last may be partial)
   int nsb0, nsb1;    // sub-bins per axis (kBinCells cells each)

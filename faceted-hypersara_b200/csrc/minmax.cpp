@@ -184,6 +184,25 @@ MinMaxAxis build_minmax_axis(int N, int K, int J, int n_samples, int n_cos) {
       ax.table_im[(size_t)(j - 1) * (n_samples + 1) + ti] = std::sin(ph) * cc[j - 1];
     }
   }
+  // polynomial fits of every tap (real and imaginary parts) over the table
+  const int nt = kPolyDegree + 1, m = n_samples + 1;
+  ax.poly.assign((size_t)J * 2 * nt, 0.0);
+  std::vector<double> V((size_t)m * nt);
+  for (int ti = 0; ti < m; ++ti) {
+    const double sv = (double)ti / n_samples - 0.5;
+    double pw = 1.0;
+    for (int k = 0; k < nt; ++k) {
+      V[ti + (size_t)m * k] = pw;
+      pw *= sv;
+    }
+  }
+  for (int j = 0; j < J; ++j)
+    for (int part = 0; part < 2; ++part) {
+      const std::vector<double>& tab = part ? ax.table_im : ax.table_re;
+      std::vector<double> t(tab.begin() + (size_t)j * m, tab.begin() + (size_t)(j + 1) * m);
+      const std::vector<double> c = lstsq(V, t, m, nt);
+      for (int k = 0; k < nt; ++k) ax.poly[((size_t)j * 2 + part) * nt + k] = c[k];
+    }
   return ax;
 }
 

@@ -11,7 +11,12 @@ struct MinMaxAxis {
   std::vector<double> scale;      // s_n, n = 0..N-1
   std::vector<double> table_re;   // h_j(dk) real part, [J][n_samples+1]
   std::vector<double> table_im;   // imaginary part
+  // degree kPolyDegree least-squares polynomials of every tap in
+  // s = (dk - J/2) - 1/2 in [-1/2, 1/2): poly[(j*2 + part)*(kPolyDegree+1) + k]
+  std::vector<double> poly;
 };
+
+constexpr int kPolyDegree = 8;
 
 // Tables for one axis: N image pixels, K grid cells, J taps.
 MinMaxAxis build_minmax_axis(int N, int K, int J, int n_samples, int n_cos = 6);
