@@ -80,6 +80,8 @@ SIGNATURES = {
     "fhs_operator_norm": (C.c_int, [_vp, C.c_int, C.c_double, _dp]),
     "fhs_update_dual_data_fidelity": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "fhs_proj_l2ball": (C.c_int, [C.c_int, C.c_int64, _dp, C.c_double, _dp, _dp]),
+    "fhs_proj_l2ball_noalloc": (C.c_int, [C.c_int, C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
     "fhs_nuclear_norm": (C.c_int, [C.c_int, C.c_int64, C.c_int, _dp, _dp]),
     "fhs_sara_n_coefs": (C.c_int64, [C.c_int, C.c_int, C.c_int]),
     "fhs_sara_analysis": (C.c_int, [C.c_int] * 5 + [_dp, _dp]),

@@ -112,6 +112,20 @@ FHS_API fhs_status fhs_update_dual_data_fidelity(fhs_measop* op, double* v2, con
 /* src/proj_l2ball.m:20-22  p = y + (x-y) min(eps/||x-y||, 1); complex n-vectors, FP64. */
 FHS_API fhs_status fhs_proj_l2ball(int device, int64_t n, const double* x, double eps, const double* y,
                            double* p);
+/* Allocation-free variant of fhs_proj_l2ball (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: code inside a
+ * CUDA stream capture, hosts whose own pool owns the device heap (MATLAB
+ * gpuArray, PyTorch's caching allocator), real-time pipelines that forbid
+ * allocation after start-up.  x, y, p are DEVICE pointers to n interleaved
+ * complex doubles; the call is enqueued on `stream` (a cudaStream_t, NULL =
+ * legacy default stream) and returns without synchronising.  Scratch: a
+ * 512 KB static device array per device that every call shares; n is limited
+ * to 134,215,680 (FHS_ERR_UNSUPPORTED above).  The first call on a device
+ * resolves the array's address (cudaGetSymbolAddress), so make it before any
+ * stream capture.  Calls that overlap on the GPU (other streams or devices'
+ * threads racing on one device) race on the scratch: serialise them. */
+FHS_API fhs_status fhs_proj_l2ball_noalloc(int device, int64_t n, const double* x, double eps,
+                                           const double* y, double* p, void* stream);
 /* src/nuclear_norm.m:25-26  sum of singular values of x reshaped [N, L]. */
 FHS_API fhs_status fhs_nuclear_norm(int device, int64_t n_pixels, int L, const double* x, double* f);
 /* SARA dictionary (op_p_sp_wlt_basis of the SARA-dictionary submodule,
