@@ -210,6 +210,197 @@ __global__ void __launch_bounds__(256) analysis_kernel(LevelArgs a, const float*
   }
 }
 
+// Fused analysis level + l21 prox.  One CTA computes a 32 (y) x 8 (x)
+// coefficient tile of one basis for every channel of a spectral group:
+//  step 1: each thread takes one input row (y) of one channel, loads its
+//          2*8+Lf-2 samples along x straight from global memory (coalesced
+//          across threads) and filters/downsamples along x in registers; the
+//          low/high outputs go to shared memory split by row parity;
+//  step 2: the owner thread of each coefficient filters along y (polyphase,
+//          conflict-free reads) for every channel, adds the dual v1 kept in
+//          registers and applies the weighted l21 prox across the group.
+// v1 is read and written once; the coefficients never reach HBM.  Grid:
+// (basis, tile, group) with the basis fastest so the 8 bases of a tile share
+// the input tile in L2.  The filter length is a template parameter (the
+// basis index selects the instantiation) so the x-filter stays in registers.
+constexpr int APH = (2 * AT0 + kSaraMaxFilter - 2 + 1) / 2;  // 39 rows per parity
+constexpr int kApChunk = 16;                                 // channels staged per phase
+
+template <int MAXL, int LF, bool LAST>
+__device__ __forceinline__ void analysis_prox_body(const LevelArgs& a, int b, int tile, int g,
+                                                   const float* __restrict__ x, float* __restrict__ apx,
+                                                   float* __restrict__ v1, const float* __restrict__ weights,
+                                                   const double* __restrict__ beta, int lg,
+                                                   double* __restrict__ l21_acc, float* sm, double* red) {
+  constexpr int IN0 = 2 * AT0 + LF - 2, IN1 = 2 * AT1 + LF - 2;
+  constexpr int CH = MAXL < kApChunk ? MAXL : kApChunk;
+  // sm layout: [CH][4 (lo_e, lo_o, hi_e, hi_o)][AT1][APH]
+  static_assert(IN0 <= 2 * APH, "row buffer too small");
+  const int n0 = a.n0[b], n1 = a.n1[b], m0 = a.m0[b], m1 = a.m1[b];
+  const int tp0 = tile % a.tiles0[b], tp1 = tile / a.tiles0[b];
+  const int p0s = tp0 * AT0, p1s = tp1 * AT1;
+  const int i0s = 2 * p0s + 2 - LF, i1s = 2 * p1s + 2 - LF;
+  const int lp0 = threadIdx.x % AT0, lp1 = threadIdx.x / AT0;
+  const int p0 = p0s + lp0, p1 = p1s + lp1;
+  const bool valid = p0 < m0 && p1 < m1;
+  const size_t o = (size_t)p1 * m0 + p0;
+  const size_t mm = (size_t)m0 * m1;
+  constexpr int NSUB = LAST ? 4 : 3;
+  const int64_t off[4] = {a.h_off[b], a.h_off[b] + (int64_t)mm, a.h_off[b] + 2 * (int64_t)mm, a.a_off[b]};
+  const float* lo_f = c_lo[b];  // uniform per CTA: constant-cache broadcast
+  const float* hi_f = c_hi[b];
+  float w[NSUB][MAXL];
+#pragma unroll
+  for (int l = 0; l < MAXL; ++l) {
+#pragma unroll
+    for (int k = 0; k < NSUB; ++k) w[k][l] = 0.f;
+    if (l < lg && valid) {
+      const float* vp = v1 + ((size_t)g * lg + l) * a.s_stride;
+#pragma unroll
+      for (int k = 0; k < NSUB; ++k) w[k][l] = vp[off[k] + o];
+    }
+  }
+#pragma unroll 1
+  for (int c0 = 0; c0 < MAXL; c0 += CH) {
+    const int nch = min(CH, lg - c0);
+    if (nch <= 0) continue;
+    // ---- step 1: x filtering of (row, channel) tasks
+    for (int task = threadIdx.x; task < IN0 * nch; task += blockDim.x) {
+      const int r = task % IN0, lc = task / IN0;
+      const size_t plane = (size_t)g * lg + c0 + lc;
+      const float* src = a.first ? x + plane * a.in_stride : apx + plane * a.apx_stride + a.in_off[b];
+      const int i0 = i0s + r;
+      float v[IN1];
+      const bool rin = i0 >= 0 && i0 < n0;
+#pragma unroll
+      for (int c = 0; c < IN1; ++c) {
+        const int i1 = i1s + c;
+        v[c] = (rin && i1 >= 0 && i1 < n1) ? src[(size_t)i1 * n0 + i0] * a.in_scale : 0.f;
+      }
+      float* base = sm + (size_t)lc * 4 * AT1 * APH;
+      const int par = r & 1, rh = r >> 1;
+#pragma unroll
+      for (int q = 0; q < AT1; ++q) {
+        float lo = 0.f, hi = 0.f;
+#pragma unroll
+        for (int t = 0; t < LF; ++t) {
+          lo = fmaf(lo_f[t], v[2 * q + LF - 1 - t], lo);
+          hi = fmaf(hi_f[t], v[2 * q + LF - 1 - t], hi);
+        }
+        base[(0 + par) * AT1 * APH + q * APH + rh] = lo;
+        base[(2 + par) * AT1 * APH + q * APH + rh] = hi;
+      }
+    }
+    __syncthreads();
+    // ---- step 2: y filtering by the owner of each coefficient
+#pragma unroll 1
+    for (int lc = 0; lc < CH; ++lc) {
+      const int l = c0 + lc;
+      if (lc < nch) {
+        const float* base = sm + (size_t)lc * 4 * AT1 * APH + lp1 * APH;
+        float aa = 0.f, hh = 0.f, vv = 0.f, dd = 0.f;
+#pragma unroll
+        for (int t = 0; t < LF; ++t) {
+          const int r = 2 * lp0 + LF - 1 - t;
+          const int par = r & 1, rh = r >> 1;
+          const float lo = base[(0 + par) * AT1 * APH + rh];
+          const float hi = base[(2 + par) * AT1 * APH + rh];
+          aa = fmaf(lo_f[t], lo, aa);
+          hh = fmaf(hi_f[t], lo, hh);
+          vv = fmaf(lo_f[t], hi, vv);
+          dd = fmaf(hi_f[t], hi, dd);
+        }
+#pragma unroll
+        for (int ll = 0; ll < MAXL; ++ll)
+          if (ll == l) {
+            w[0][ll] += hh;
+            w[1][ll] += vv;
+            w[2][ll] += dd;
+            if constexpr (LAST) w[NSUB - 1][ll] += aa;
+          }
+        if (!LAST && valid) apx[((size_t)g * lg + l) * a.apx_stride + a.a_off[b] + o] = aa;
+      }
+    }
+    __syncthreads();
+  }
+  double l21 = 0.0;
+  if (valid) {
+    const float bt = (float)beta[g];
+    const float* wg = weights + (size_t)g * a.s_stride;
+#pragma unroll
+    for (int k = 0; k < NSUB; ++k) {
+      float ss = 0.f;
+#pragma unroll
+      for (int l = 0; l < MAXL; ++l)
+        if (l < lg) ss = fmaf(w[k][l], w[k][l], ss);
+      const float l2 = sqrtf(ss);
+      l21 += l2;
+      const float soft = fmaxf(l2 - bt * wg[off[k] + o], 0.f) / (l2 + 2.220446049250313e-16f);
+#pragma unroll
+      for (int l = 0; l < MAXL; ++l)
+        if (l < lg) v1[((size_t)g * lg + l) * a.s_stride + off[k] + o] = w[k][l] - soft * w[k][l];
+    }
+  }
+  if (l21_acc) {
+    for (int sh = 16; sh > 0; sh >>= 1) l21 += __shfl_down_sync(0xffffffffu, l21, sh);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l21;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int i = 0; i < 8; ++i) t += red[i];
+      atomicAdd(l21_acc + g, t);
+    }
+  }
+}
+
+template <int MAXL>
+__global__ void __launch_bounds__(256, (MAXL > 16 ? 1 : 2)) analysis_prox_kernel(LevelArgs a, const float* __restrict__ x,
+                                                            float* __restrict__ apx, float* __restrict__ v1,
+                                                            const float* __restrict__ weights,
+                                                            const double* __restrict__ beta, int lg,
+                                                            double* __restrict__ l21_acc) {
+  extern __shared__ float sm_ap[];
+  __shared__ double red[8];
+  const int b = blockIdx.x, tile = blockIdx.y, g = blockIdx.z;
+  if (tile >= a.tiles[b]) return;
+  if (a.last) {
+    switch (b) {
+#define FHS_C(BB, LFV) \
+  case BB: analysis_prox_body<MAXL, LFV, true>(a, b, tile, g, x, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); break;
+      FHS_C(0, 2) FHS_C(1, 4) FHS_C(2, 6) FHS_C(3, 8) FHS_C(4, 10) FHS_C(5, 12) FHS_C(6, 14) FHS_C(7, 16)
+#undef FHS_C
+    }
+  } else {
+    switch (b) {
+#define FHS_C(BB, LFV) \
+  case BB: analysis_prox_body<MAXL, LFV, false>(a, b, tile, g, x, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); break;
+      FHS_C(0, 2) FHS_C(1, 4) FHS_C(2, 6) FHS_C(3, 8) FHS_C(4, 10) FHS_C(5, 12) FHS_C(6, 14) FHS_C(7, 16)
+#undef FHS_C
+    }
+  }
+}
+
+template <int MAXL>
+size_t analysis_prox_smem() {
+  constexpr int CH = MAXL < kApChunk ? MAXL : kApChunk;
+  return (size_t)CH * 4 * AT1 * APH * sizeof(float);
+}
+
+template <int MAXL>
+void launch_analysis_prox(dim3 grid, cudaStream_t s, const LevelArgs& a, const float* x, float* apx, float* v1,
+                          const float* weights, const double* beta, int lg, double* l21_acc) {
+  const size_t smem = analysis_prox_smem<MAXL>();
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (smem > 48 * 1024 && dev < 64 && !attr[dev]) {
+    FHS_CUDA(cudaFuncSetAttribute(analysis_prox_kernel<MAXL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    attr[dev] = true;
+  }
+  analysis_prox_kernel<MAXL><<<grid, 256, smem, s>>>(a, x, apx, v1, weights, beta, lg, l21_acc);
+}
+
 // ----------------------------------------------------------- synthesis
 constexpr int ST0 = 32, ST1 = 16;                          // output tile (y, x)
 constexpr int SP0 = ST0 / 2 + kSaraMaxFilter / 2;          // 24 coefficient rows
@@ -338,12 +529,14 @@ __global__ void __launch_bounds__(256) l21_prox_kernel(float* __restrict__ v1, c
                                                        const float* __restrict__ weights,
                                                        const double* __restrict__ beta, int64_t s,
                                                        int64_t dirac_off, int64_t npix, int lg,
-                                                       double* __restrict__ l21_partials) {
+                                                       double* __restrict__ l21_partials, int64_t i_begin,
+                                                       double* __restrict__ l21_acc) {
   const int g = blockIdx.y;
   const float bt = (float)beta[g];
   const float* wg = weights + (size_t)g * s;
   double l21 = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s; i += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = i_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s;
+       i += (int64_t)gridDim.x * blockDim.x) {
     float w[MAXL];
     float ss = 0.f;
 #pragma unroll
@@ -362,7 +555,7 @@ __global__ void __launch_bounds__(256) l21_prox_kernel(float* __restrict__ v1, c
     for (int l = 0; l < MAXL; ++l)
       if (l < lg) v1[((size_t)g * lg + l) * s + i] = w[l] - soft * w[l];
   }
-  if (l21_partials) {
+  if (l21_partials || l21_acc) {
     __shared__ double red[256];
     red[threadIdx.x] = l21;
     __syncthreads();
@@ -370,7 +563,10 @@ __global__ void __launch_bounds__(256) l21_prox_kernel(float* __restrict__ v1, c
       if (threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
       __syncthreads();
     }
-    if (threadIdx.x == 0) l21_partials[(size_t)g * gridDim.x + blockIdx.x] = red[0];
+    if (threadIdx.x == 0) {
+      if (l21_partials) l21_partials[(size_t)g * gridDim.x + blockIdx.x] = red[0];
+      if (l21_acc) atomicAdd(l21_acc + g, red[0]);
+    }
   }
 }
 
@@ -464,6 +660,71 @@ void sara_analysis(const SaraPlan& p, const float* x, float* coef, float* apx, i
   }
 }
 
+bool sara_fused_supported(int lg) { return lg >= 1 && lg <= 32; }
+
+void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* apx, const float* weights,
+                        const double* beta, int n_groups, int lg, double* l21_acc, cudaStream_t s) {
+  upload_filters();
+  FHS_CHECK(sara_fused_supported(lg), FHS_ERR_UNSUPPORTED, "fused SARA prox supports at most 32 channels per group");
+  for (int j = 1; j <= p.J; ++j) {
+    LevelArgs a{};
+    int maxt = 0;
+    for (int b = 0; b < kSaraWavelets; ++b) {
+      a.n0[b] = p.n0[b][j - 1];
+      a.n1[b] = p.n1[b][j - 1];
+      a.m0[b] = p.n0[b][j];
+      a.m1[b] = p.n1[b][j];
+      a.tiles0[b] = ceil_div(a.m0[b], AT0);
+      a.tiles[b] = a.tiles0[b] * ceil_div(a.m1[b], AT1);
+      maxt = std::max(maxt, a.tiles[b]);
+      a.in_off[b] = j > 1 ? p.apx_off[b][j - 1] : 0;
+      a.a_off[b] = j == p.J ? p.offA[b] : p.apx_off[b][j];
+      a.h_off[b] = p.offH[b][j];
+    }
+    a.in_stride = (int64_t)p.Ny * p.Nx;
+    a.s_stride = p.s;
+    a.apx_stride = p.apx_total;
+    a.first = j == 1;
+    a.last = j == p.J;
+    a.in_scale = j == 1 ? 1.f / 3.f : 1.f;
+    dim3 grid(kSaraWavelets, maxt, n_groups);
+#define FHS_AP(MAXL) launch_analysis_prox<MAXL>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc)
+    if (lg <= 1)
+      FHS_AP(1);
+    else if (lg <= 4)
+      FHS_AP(4);
+    else if (lg <= 8)
+      FHS_AP(8);
+    else if (lg <= 16)
+      FHS_AP(16);
+    else
+      FHS_AP(32);
+#undef FHS_AP
+    count_launch();
+    FHS_LAUNCH_CHECK();
+  }
+  // Dirac part: coefficients are xhat/3
+  const int64_t npix = (int64_t)p.Ny * p.Nx;
+  const int64_t off = p.boff[kSaraWavelets];
+  dim3 grid(nblk(npix), n_groups);
+#define FHS_DP(MAXL)                                                                                            \
+  l21_prox_kernel<MAXL><<<grid, 256, 0, s>>>(v1, nullptr, xhat, weights, beta, p.s, off, npix, lg, nullptr, off, \
+                                             l21_acc)
+  if (lg <= 1)
+    FHS_DP(1);
+  else if (lg <= 4)
+    FHS_DP(4);
+  else if (lg <= 8)
+    FHS_DP(8);
+  else if (lg <= 16)
+    FHS_DP(16);
+  else
+    FHS_DP(32);
+#undef FHS_DP
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
 void sara_dirac(const SaraPlan& p, const float* x, float* coef, int np, cudaStream_t s) {
   const int64_t npix = (int64_t)p.Ny * p.Nx;
   dirac_kernel<<<dim3(nblk(npix), np), 256, 0, s>>>(x, coef, p.s, p.boff[kSaraWavelets], npix);
@@ -509,7 +770,8 @@ void sara_l21_prox(const SaraPlan& p, float* v1, const float* coef, const float*
   dim3 grid(nblk(p.s), n_groups);
   const int64_t off = p.boff[kSaraWavelets];
 #define FHS_L21(MAXL)                                                                                       \
-  l21_prox_kernel<MAXL><<<grid, 256, 0, s>>>(v1, coef, xhat, weights, beta, p.s, off, npix, lg, l21_partials)
+  l21_prox_kernel<MAXL><<<grid, 256, 0, s>>>(v1, coef, xhat, weights, beta, p.s, off, npix, lg, l21_partials, 0, \
+                                             nullptr)
   if (lg <= 1)
     FHS_L21(1);
   else if (lg <= 4)

@@ -43,6 +43,13 @@ void sara_dirac(const SaraPlan& p, const float* x, float* coef, int np, cudaStre
 // l21 (optional, [n_groups] FP64): sum over coefficients of l2.
 void sara_l21_prox(const SaraPlan& p, float* v1, const float* coef, const float* xhat, const float* weights,
                    const double* beta, int n_groups, int lg, double* l21_partials, cudaStream_t s);
+// Fused analysis + weighted l21 prox of every level and of the Dirac part
+// (coefficients never written): v1 <- prox(v1 + Psit xhat) per group of lg
+// (<= 32) channels.  l21_acc[g] (FP64, zeroed by the caller) receives
+// sum_i ||v1_i + (Psit xhat)_i||_2.
+bool sara_fused_supported(int lg);
+void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* apx, const float* weights,
+                        const double* beta, int n_groups, int lg, double* l21_acc, cudaStream_t s);
 // Row l2 norms over a group of the analysis coefficients (coef + Dirac from
 // x): out[g][i] = ||coef_i||.  Used for weights and prior values.
 void sara_row_norms(const SaraPlan& p, const float* coef, const float* x, int n_groups, int lg, float* out,

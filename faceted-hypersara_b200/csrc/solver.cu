@@ -134,7 +134,8 @@ __global__ void stats_kernel(const double* __restrict__ primal_part, int nparts,
                              const double* __restrict__ blk_stats, const int32_t* __restrict__ ch_nblk,
                              const int32_t* __restrict__ ch_blkoff, const double* __restrict__ blk_eps,
                              const double* __restrict__ nuc_vals, int Q, const double* __restrict__ l21_part,
-                             int prox_blocks, double* __restrict__ ring, int* __restrict__ counter) {
+                             int prox_blocks, const double* __restrict__ l21_acc, double* __restrict__ ring,
+                             int* __restrict__ counter) {
   __shared__ int c;
   if (threadIdx.x == 0) c = *counter;
   __syncthreads();
@@ -155,6 +156,7 @@ __global__ void stats_kernel(const double* __restrict__ primal_part, int nparts,
     if (nuc_vals)
       for (int q = 0; q < Q; ++q) nu += nuc_vals[g * Q + q];
     for (int k = 0; k < prox_blocks; ++k) l21 += l21_part[(size_t)g * prox_blocks + k];
+    l21 += l21_acc[g];
     rec[g * kReportFields + 0] = rx;
     rec[g * kReportFields + 1] = nx;
     rec[g * kReportFields + 2] = r2;
@@ -210,7 +212,7 @@ Solver::~Solver() {
 }
 
 static const char* kStageNames[] = {"primal_pad", "fft_forward", "degrid_dual", "block_reduce", "grid_dual",
-                                    "fft_inverse", "sara_analysis", "l21_prox", "sara_synthesis", "facet_gram",
+                                    "fft_inverse", "sara_analysis_prox", "l21_prox", "sara_synthesis", "facet_gram",
                                     "facet_eig", "facet_reconstruct", "assemble_g", "stats"};
 constexpr int kStages = sizeof(kStageNames) / sizeof(kStageNames[0]);
 
@@ -239,9 +241,15 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   mark();
   fft_inverse(op, 0, L, s);
   mark();
-  sara_analysis(S->sp, S->xhat.p, S->coef.p, S->apx.p, L, s);
-  mark();
-  sara_l21_prox(S->sp, S->v1.p, S->coef.p, S->xhat.p, S->w1.p, S->beta1.p, S->G, S->lg, S->l21_part.p, s);
+  FHS_CUDA(cudaMemsetAsync(S->l21_acc.p, 0, S->G * sizeof(double), s));
+  if (sara_fused_supported(S->lg)) {
+    sara_analysis_prox(S->sp, S->xhat.p, S->v1.p, S->apx.p, S->w1.p, S->beta1.p, S->G, S->lg, S->l21_acc.p, s);
+    mark();
+  } else {
+    sara_analysis(S->sp, S->xhat.p, S->coef.p, S->apx.p, L, s);
+    mark();
+    sara_l21_prox(S->sp, S->v1.p, S->coef.p, S->xhat.p, S->w1.p, S->beta1.p, S->G, S->lg, S->l21_part.p, s);
+  }
   mark();
   sara_synthesis(S->sp, S->v1.p, S->g1.p, S->apx.p, L, (float)S->sigma11, s);
   mark();
@@ -273,7 +281,8 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   mark();
   stats_kernel<<<1, 64, 0, s>>>(S->primal_part.p, kPrimalBlocks, S->lg, S->G, op->blk_stats.p, op->ch_nblk.p,
                                 op->ch_blkoff.p, op->blk_eps.p, S->nuclear ? S->nuc_vals.p : nullptr,
-                                S->nuclear ? S->np.Q : 0, S->l21_part.p, S->prox_blocks, S->ring.p,
+                                S->nuclear ? S->np.Q : 0, S->l21_part.p,
+                                sara_fused_supported(S->lg) ? 0 : S->prox_blocks, S->l21_acc.p, S->ring.p,
                                 S->ring_counter.p);
   count_launch();
   FHS_LAUNCH_CHECK();
@@ -404,7 +413,7 @@ fhs_status fhs_solver_create(fhs_measop* op_, const fhs_solver_config* cfg, fhs_
     S->g.alloc(L * N);
     S->xhat.alloc(L * N);
     S->g1.alloc(L * N);
-    S->coef.alloc(L * sc);
+    S->coef.alloc(L * sc);  // analysis output for weights (and the unfused prox path)
     S->apx.alloc(L * S->sp.apx_total);
     S->v1.alloc(L * sc);
     S->w1.alloc((size_t)S->G * sc);
@@ -426,6 +435,8 @@ fhs_status fhs_solver_create(fhs_measop* op_, const fhs_solver_config* cfg, fhs_
     S->primal_part.alloc(L * kPrimalBlocks * 2);
     S->prox_blocks = nblk(sc);
     S->l21_part.alloc((size_t)S->G * S->prox_blocks);
+    S->l21_acc.alloc(S->G);
+    S->l21_acc.zero(s);
     S->ring.alloc((size_t)kReportRing * S->G * kReportFields);
     S->ring_counter.alloc(1);
     FHS_CUDA(cudaStreamSynchronize(s));

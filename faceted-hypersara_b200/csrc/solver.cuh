@@ -23,7 +23,8 @@ struct Solver {
   DevBuf<float2> y, v2, gold;
   DevBuf<float> sigma22;
   DevBuf<double> primal_part;   // [L][kPrimalBlocks][2]
-  DevBuf<double> l21_part;      // [G][prox blocks]
+  DevBuf<double> l21_part;      // [G][prox blocks] (unfused prox path)
+  DevBuf<double> l21_acc;       // [G] sum of row norms (fused path)
   DevBuf<double> nuc_vals;      // [G][Q]
   DevBuf<double> ring;          // [kReportRing][G][kReportFields]
   DevBuf<int> ring_counter;
