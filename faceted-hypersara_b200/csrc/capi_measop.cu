@@ -131,6 +131,8 @@ fhs_status fhs_scaled_fft_adjoint(fhs_measop* op_, const double* Fx, double* xc)
     launch_grid_from_matlab(st, op->gridB.p, op->Ny, op->Nx, op->Ky, op->Kx, 1, s);
     fft_inverse(op, 0, 1, s);
     launch_crop_complex(op->gridA.p, st, op->sy.p, op->sx.p, op->Ny, op->Nx, op->Ky, op->Kx, 1, s);
+    // the gridding kernels never write empty tiles: restore the zeros of plane 0
+    FHS_CUDA(cudaMemsetAsync(op->gridB.p, 0, No * sizeof(float2), s));
     FHS_CUDA(cudaMemcpyAsync(xc, st, 2 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
     FHS_CUDA(cudaStreamSynchronize(s));
   });

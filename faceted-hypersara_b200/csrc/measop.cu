@@ -21,9 +21,10 @@
 //
 // Degridding: one CTA per 64x64 grid tile stages the tile and its (J-1)-cell
 // apron in shared memory and gathers the taps of the visibilities that start
-// in the tile.  Gridding: one CTA per tile accumulates, in shared memory, the
-// taps of the visibilities that start in the tile or in the 8-cell ring below
-// it, then writes the tile once: no global atomics, no grid zeroing.
+// in the tile.  Gridding: one CTA per tile accumulates, in warp-private
+// shared-memory bands, the taps of the visibilities that start in the tile
+// or in the 8-cell ring below it, then writes the tile once: no atomics of
+// any kind, no grid zeroing.
 #include "measop.cuh"
 
 #include <algorithm>
@@ -74,7 +75,9 @@ __device__ __forceinline__ int wrap(int k, int K) {
 
 // ---------------------------------------------------------------- degrid
 template <int J, bool DUAL>
-__global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid, int c0,
+__global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid,
+                                                     const WorkItem* __restrict__ items,
+                                                     const int* __restrict__ order, int item0,
                                                      float2* __restrict__ out, const float2* __restrict__ v2,
                                                      float2* __restrict__ gold,
                                                      const float2* __restrict__ y,
@@ -84,19 +87,17 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
   constexpr int R = kTileCells + J - 1;
   __shared__ float2 sm[R * P];
   __shared__ double bacc[kMaxBlocksPerChannel * 2];
-  const int tile = blockIdx.x;
-  const int ch = c0 + blockIdx.y;
+  const WorkItem it = items[order ? order[blockIdx.x] : item0 + blockIdx.x];
+  const int tile = it.tile;
+  const int ch = it.ch;
   const int t0 = tile % op.nT0, t1 = tile / op.nT0;
   const int32_t* off = op.sb_off + (size_t)ch * (op.nkeys + 1);
-  const int beg = off[tile * kSubPerTile * kSubPerTile];
-  const int end = off[(tile + 1) * kSubPerTile * kSubPerTile];
+  const int tb = off[tile * kSubPerTile * kSubPerTile];
+  const int te = off[(tile + 1) * kSubPerTile * kSubPerTile];
+  const int beg = tb + (int)(((int64_t)(te - tb) * it.split) / it.nsplit);
+  const int end = tb + (int)(((int64_t)(te - tb) * (it.split + 1)) / it.nsplit);
   if (DUAL) {
     if (threadIdx.x < kMaxBlocksPerChannel * 2) bacc[threadIdx.x] = 0.0;
-  }
-  if (beg == end) {
-    if (DUAL && threadIdx.x < kMaxBlocksPerChannel * 2)
-      partials[((size_t)blockIdx.y * gridDim.x + tile) * kMaxBlocksPerChannel * 2 + threadIdx.x] = 0.0;
-    return;
   }
   const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
   const float2* g = grid + (size_t)ch * op.Ky * op.Kx;
@@ -143,122 +144,258 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
   if (DUAL) {
     __syncthreads();
     if (threadIdx.x < kMaxBlocksPerChannel * 2)
-      partials[((size_t)blockIdx.y * gridDim.x + tile) * kMaxBlocksPerChannel * 2 + threadIdx.x] =
-          bacc[threadIdx.x];
+      partials[(size_t)it.slot * kMaxBlocksPerChannel * 2 + threadIdx.x] = bacc[threadIdx.x];
   }
 }
 
 // ------------------------------------------------------------------ grid
-struct Range {
+// One CTA per 64x64 grid tile and channel, 9 warps.  Warp w owns the
+// visibilities whose start column lies in band w (band 0: the 8 columns left
+// of the tile; bands 1-8: the tile's own 8-column strips), including those
+// whose start row lies in the 8 rows above the tile, and accumulates their
+// taps into a private 14-column x 64-row buffer: no atomics, no other warp
+// writes there.  Per chunk of 32 visibilities every lane evaluates the tap
+// polynomials of one visibility and stages conj(hy) and conj(hx) w v in
+// shared memory; the warp then walks the chunk one visibility at a time with
+// one lane per tap (two rounds for the 49 taps); complex accumulators with a
+// pitch of 71 (= 7 mod 32) keep each half-warp's 64-bit accesses on distinct
+// banks.  The bands are summed into the tile at the end and the tile is
+// written once.
+constexpr int kBands = kSubPerTile + 1;         // 9
+constexpr int kBandCols = kBinCells + kMaxTaps - 2;  // 14 columns covered by a band
+constexpr int kAccPitch = kTileCells + 7;       // 71
+
+struct BandRange {
   int beg, end;
-  int ring0, ring1;
+  int ring0;  // start rows above the tile (wrap-adjusted offsets)
 };
 
-__device__ __forceinline__ int sb_key(const OpView& op, int sb0, int sb1) {
-  return ((sb1 / kSubPerTile) * op.nT0 + sb0 / kSubPerTile) * (kSubPerTile * kSubPerTile) +
-         (sb1 % kSubPerTile) * kSubPerTile + (sb0 % kSubPerTile);
-}
-
 template <int J, bool DUAL>
-__global__ void __launch_bounds__(256) grid_kernel(OpView op, float2* __restrict__ gridB, int c0,
-                                                   const float2* __restrict__ vin,
-                                                   float2* __restrict__ v2,
-                                                   const float* __restrict__ blk_scale,
-                                                   const float2* __restrict__ zbuf) {
-  __shared__ float acc_re[kTileCells * kSmemPitch];
-  __shared__ float acc_im[kTileCells * kSmemPitch];
-  __shared__ Range rng[2 + 2 * kSubPerTile];
-  __shared__ int nrng;
-  __shared__ int total;
-  const int tile = blockIdx.x;
-  const int ch = c0 + blockIdx.y;
+__global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __restrict__ gridB,
+                                                           const WorkItem* __restrict__ items,
+                                                           const int* __restrict__ order, int item0,
+                                                           float2* __restrict__ partial,
+                                                           const float2* __restrict__ vin,
+                                                           float2* __restrict__ v2,
+                                                           const float* __restrict__ blk_scale,
+                                                           const float2* __restrict__ zbuf) {
+  static_assert(J <= kMaxTaps && J * J <= 64, "two tap rounds per visibility");
+  extern __shared__ float2 gsm2[];
+  float2* acc = gsm2;                                           // [kBands][kBandCols][kAccPitch]
+  float2* stage = acc + kBands * kBandCols * kAccPitch;         // [kBands][32][2J]
+  int2* stage_d = reinterpret_cast<int2*>(stage + kBands * 32 * 2 * J);  // [kBands][32]
+  __shared__ BandRange rng[kBands][2];
+  __shared__ int any;
+  const WorkItem it = items[order ? order[blockIdx.x] : item0 + blockIdx.x];
+  const int tile = it.tile;
+  const int ch = it.ch;
   const int t0 = tile % op.nT0, t1 = tile / op.nT0;
   const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
   const int T0 = min(kTileCells, op.Ky - a0), T1 = min(kTileCells, op.Kx - a1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t* off = op.sb_off + (size_t)ch * (op.nkeys + 1);
-  for (int i = threadIdx.x; i < kTileCells * kSmemPitch; i += blockDim.x) {
-    acc_re[i] = 0.f;
-    acc_im[i] = 0.f;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  if (lane == 0) {
+    // band 0 = the sub-bin column left of the tile (wraps), bands 1-8 = the tile's columns
+    const int sbr0 = (t0 * kSubPerTile - 1 + op.nsb0) % op.nsb0;  // sub-bin row above the tile
+    const int nrows = min(kSubPerTile, op.nsb0 - t0 * kSubPerTile);
+    int sb1;
+    bool ok = true;
+    if (warp == 0) {
+      sb1 = (t1 * kSubPerTile - 1 + op.nsb1) % op.nsb1;
+    } else {
+      sb1 = t1 * kSubPerTile + warp - 1;
+      ok = sb1 < op.nsb1;
+    }
+    BandRange r0{0, 0, 0}, r1{0, 0, 1};
+    if (ok) {
+      const int base =
+          ((sb1 / kSubPerTile) * op.nT0 + t0) * (kSubPerTile * kSubPerTile) + (sb1 % kSubPerTile) * kSubPerTile;
+      r0.beg = off[base];
+      r0.end = off[base + nrows];
+      const int kr = ((sb1 / kSubPerTile) * op.nT0 + sbr0 / kSubPerTile) * (kSubPerTile * kSubPerTile) +
+                     (sb1 % kSubPerTile) * kSubPerTile + (sbr0 % kSubPerTile);
+      r1.beg = off[kr];
+      r1.end = off[kr + 1];
+    }
+    // this item's slice of both ranges
+    auto slice = [&](BandRange r) {
+      const int len = r.end - r.beg;
+      BandRange q = r;
+      q.beg = r.beg + (int)(((int64_t)len * it.split) / it.nsplit);
+      q.end = r.beg + (int)(((int64_t)len * (it.split + 1)) / it.nsplit);
+      return q;
+    };
+    r0 = slice(r0);
+    r1 = slice(r1);
+    rng[warp][0] = r0;
+    rng[warp][1] = r1;
+    if (r0.end > r0.beg || r1.end > r1.beg) atomicOr(&any, 1);
   }
-  if (threadIdx.x == 0) {
-    int n = 0;
-    const int kb = tile * kSubPerTile * kSubPerTile;
-    rng[n++] = Range{off[kb], off[kb + kSubPerTile * kSubPerTile], 0, 0};
-    const int sbc0 = (t0 * kSubPerTile - 1 + op.nsb0) % op.nsb0;
-    const int sbr1 = (t1 * kSubPerTile - 1 + op.nsb1) % op.nsb1;
-    const int sb1_end = min(t1 * kSubPerTile + kSubPerTile, op.nsb1);
-    const int sb0_end = min(t0 * kSubPerTile + kSubPerTile, op.nsb0);
-    for (int sb1 = t1 * kSubPerTile; sb1 < sb1_end; ++sb1) {
-      const int k = sb_key(op, sbc0, sb1);
-      if (off[k + 1] > off[k]) rng[n++] = Range{off[k], off[k + 1], 1, 0};
-    }
-    {
-      const int k = sb_key(op, t0 * kSubPerTile, sbr1);
-      const int k2 = sb_key(op, sb0_end - 1, sbr1) + 1;
-      if (off[k2] > off[k]) rng[n++] = Range{off[k], off[k2], 0, 1};
-    }
-    {
-      const int k = sb_key(op, sbc0, sbr1);
-      if (off[k + 1] > off[k]) rng[n++] = Range{off[k], off[k + 1], 1, 1};
-    }
-    int tot = 0;
-    for (int r = 0; r < n; ++r) tot += rng[r].end - rng[r].beg;
-    nrng = n;
-    total = tot;
+  __syncthreads();
+  // split tiles write a partial tile (summed by grid_combine_kernel)
+  float2* gb;
+  size_t ld;  // leading dimension of the destination
+  int g0, g1;
+  if (it.slot >= 0) {
+    gb = partial + (size_t)it.slot * kTileCells * kTileCells;
+    ld = kTileCells;
+    g0 = 0;
+    g1 = 0;
+  } else {
+    gb = gridB + (size_t)ch * op.Ky * op.Kx;
+    ld = op.Ky;
+    g0 = a0;
+    g1 = a1;
   }
+  if (!any) {
+    for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
+      const int cc1 = idx / T0, cc0 = idx - cc1 * T0;
+      gb[(size_t)(g1 + cc1) * ld + g0 + cc0] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < kBands * kBandCols * kAccPitch; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
   __syncthreads();
   const int64_t vo = op.ch_voff[ch];
   const float* scl = DUAL ? blk_scale + (size_t)ch * kMaxBlocksPerChannel : nullptr;
-  for (int it = threadIdx.x; it < total; it += blockDim.x) {
-    int r = 0, rem = it;
-    while (rem >= rng[r].end - rng[r].beg) {
-      rem -= rng[r].end - rng[r].beg;
-      ++r;
-    }
-    const int i = rng[r].beg + rem;
-    const float4 gm = __ldg(op.geom + vo + i);
-    const unsigned kp = __float_as_uint(gm.z);
-    int d0 = (int)(kp & 0x3FFFu) - a0;
-    int d1 = (int)((kp >> 14) & 0x3FFFu) - a1;
-    if (rng[r].ring0 && d0 >= 0) d0 -= op.Ky;
-    if (rng[r].ring1 && d1 >= 0) d1 -= op.Kx;
-    const bool own = (r == 0);
-    float2 v;
-    if (DUAL) {
-      const float2 z = zbuf[vo + i];
-      const float sc = scl[kp >> 28];
-      v = make_float2(z.x * sc, z.y * sc);
-      if (own) v2[vo + i] = v;
-    } else {
-      v = vin[vo + i];
-    }
-    if (d0 + J <= 0 || d0 >= T0 || d1 + J <= 0 || d1 >= T1) continue;
-    float2 hy[J], hx[J];
-    taps<J>(op.py, gm.x, hy);
-    taps<J>(op.px, gm.y, hx);
-    v.x *= gm.w;
-    v.y *= gm.w;
+  const int xb = warp == 0 ? -kBinCells : (warp - 1) * kBinCells;  // first tile column of the band buffer
+  float2* ab = acc + warp * kBandCols * kAccPitch;
+  float2* st = stage + warp * 32 * 2 * J;
+  int2* sd = stage_d + warp * 32;
+  // per-lane tap constants of the two rounds
+  int jyA, jxA, jyB, jxB;
+  {
+    const int tA = lane, tB = lane + 32;
+    jxA = tA / J;
+    jyA = tA - jxA * J;
+    jxB = tB / J;
+    jyB = tB - jxB * J;
+  }
+  const bool hasB = lane + 32 < J * J;
+  const int offA = jxA * kAccPitch + jyA, offB = jxB * kAccPitch + jyB;
+  for (int part = 0; part < 2; ++part) {
+    const BandRange r = rng[warp][part];
+    for (int base = r.beg; base < r.end; base += 32) {
+      const int n = min(32, r.end - base);
+      if (lane < n) {
+        const int i = base + lane;
+        const float4 gm = __ldg(op.geom + vo + i);
+        const unsigned kp = __float_as_uint(gm.z);
+        int d0 = (int)(kp & 0x3FFFu) - a0;
+        int d1 = (int)((kp >> 14) & 0x3FFFu) - a1;
+        if (r.ring0 && d0 >= 0) d0 -= op.Ky;
+        if (warp == 0 && d1 >= 0) d1 -= op.Kx;
+        float2 v;
+        if (DUAL) {
+          const float2 z = zbuf[vo + i];
+          const float sc = scl[kp >> 28];
+          v = make_float2(z.x * sc, z.y * sc);
+          if (part == 0 && warp > 0) v2[vo + i] = v;  // the owner tile writes the dual
+        } else {
+          v = vin[vo + i];
+        }
+        v.x *= gm.w;
+        v.y *= gm.w;
+        float2 hy[J], hx[J];
+        taps<J>(op.py, gm.x, hy);
+        taps<J>(op.px, gm.y, hx);
 #pragma unroll
-    for (int jx = 0; jx < J; ++jx) {
-      const int c1 = d1 + jx;
-      if ((unsigned)c1 >= (unsigned)T1) continue;
-      const float2 t = cmulc(hx[jx], v);
-#pragma unroll
-      for (int jy = 0; jy < J; ++jy) {
-        const int cc0 = d0 + jy;
-        if ((unsigned)cc0 >= (unsigned)T0) continue;
-        const float2 a = cmulc(hy[jy], t);
-        atomicAdd(&acc_re[c1 * kSmemPitch + cc0], a.x);
-        atomicAdd(&acc_im[c1 * kSmemPitch + cc0], a.y);
+        for (int j = 0; j < J; ++j) {
+          st[lane * 2 * J + j] = make_float2(hy[j].x, -hy[j].y);   // conj(hy)
+          st[lane * 2 * J + J + j] = cmulc(hx[j], v);               // conj(hx) w v
+        }
+        sd[lane] = make_int2(d0, d1 - xb);
+      }
+      __syncwarp();
+      for (int k = 0; k < n; ++k) {
+        const int2 d = sd[k];                 // (row offset, band column offset)
+        const float2* sk = st + k * 2 * J;
+        const int a = d.y * kAccPitch + d.x;  // accumulator index of tap (0, 0)
+        const int tc = d.y + xb;              // tile column of tap (0, 0)
+        if ((unsigned)(d.x + jyA) < (unsigned)T0 && (unsigned)(tc + jxA) < (unsigned)T1) {
+          const float2 val = cmul(sk[jyA], sk[J + jxA]);
+          float2 o = ab[a + offA];
+          o.x += val.x;
+          o.y += val.y;
+          ab[a + offA] = o;
+        }
+        if (hasB && (unsigned)(d.x + jyB) < (unsigned)T0 && (unsigned)(tc + jxB) < (unsigned)T1) {
+          const float2 val = cmul(sk[jyB], sk[J + jxB]);
+          float2 o = ab[a + offB];
+          o.x += val.x;
+          o.y += val.y;
+          ab[a + offB] = o;
+        }
+        __syncwarp();
       }
     }
   }
   __syncthreads();
-  float2* gb = gridB + (size_t)ch * op.Ky * op.Kx;
   for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
-    const int c1 = idx / T0, cc0 = idx - c1 * T0;
-    gb[(size_t)(a1 + c1) * op.Ky + a0 + cc0] =
-        make_float2(acc_re[c1 * kSmemPitch + cc0], acc_im[c1 * kSmemPitch + cc0]);
+    const int c = idx / T0, rr = idx - c * T0;
+    const int w1 = c / kBinCells + 1;      // band whose own strip holds column c
+    float2 val = acc[w1 * kBandCols * kAccPitch + (c - (w1 - 1) * kBinCells) * kAccPitch + rr];
+    const int w0 = w1 - 1;                 // the band to the left reaches 6 columns into the strip
+    const int cl = c - (w0 == 0 ? -kBinCells : (w0 - 1) * kBinCells);
+    if (cl < kBandCols) {
+      const float2 o = acc[w0 * kBandCols * kAccPitch + cl * kAccPitch + rr];
+      val.x += o.x;
+      val.y += o.y;
+    }
+    gb[(size_t)(g1 + c) * ld + g0 + rr] = val;
+  }
+}
+
+// Sums the partial tiles of split tiles into the grid (fixed order: deterministic).
+__global__ void __launch_bounds__(256) grid_combine_kernel(OpView op, float2* __restrict__ gridB,
+                                                           const GridCombine* __restrict__ comb,
+                                                           const float2* __restrict__ partial) {
+  const GridCombine c = comb[blockIdx.x];
+  const int t0 = c.tile % op.nT0, t1 = c.tile / op.nT0;
+  const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
+  const int T0 = min(kTileCells, op.Ky - a0), T1 = min(kTileCells, op.Kx - a1);
+  float2* gb = gridB + (size_t)c.ch * op.Ky * op.Kx;
+  for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
+    const int cc1 = idx / T0, cc0 = idx - cc1 * T0;
+    float2 v = make_float2(0.f, 0.f);
+    for (int k = 0; k < c.nsplit; ++k) {
+      const float2 p = partial[(size_t)(c.pbase + k) * kTileCells * kTileCells + (size_t)cc1 * kTileCells + cc0];
+      v.x += p.x;
+      v.y += p.y;
+    }
+    gb[(size_t)(a1 + cc1) * op.Ky + a0 + cc0] = v;
+  }
+}
+
+constexpr size_t kGridSmem = kBands * kBandCols * kAccPitch * sizeof(float2) +
+                             kBands * 32 * 2 * kMaxTaps * sizeof(float2) + kBands * 32 * sizeof(int2);
+
+template <int J, bool DUAL>
+void launch_grid_kernel(const MeasOp* op, int c0, int nc, const float2* vin, float2* v2, const float* scale,
+                        const float2* zbuf, cudaStream_t s) {
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr[dev]) {
+    FHS_CUDA(cudaFuncSetAttribute(grid_kernel<J, DUAL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kGridSmem));
+    attr[dev] = true;
+  }
+  const int i0 = op->h_gr_off[c0], n = op->h_gr_off[c0 + nc] - i0;
+  if (n > 0) {
+    grid_kernel<J, DUAL><<<n, kBands * 32, kGridSmem, s>>>(op->view(), op->gridB.p, op->gr_items.p,
+                                                           nullptr, i0, op->gr_partial.p,
+                                                           vin, v2, scale, zbuf);
+    count_launch();
+    FHS_LAUNCH_CHECK();
+  }
+  const int k0 = op->h_comb_off[c0], nk = op->h_comb_off[c0 + nc] - k0;
+  if (nk > 0) {
+    grid_combine_kernel<<<nk, 256, 0, s>>>(op->view(), op->gridB.p, op->gr_combine.p + k0, op->gr_partial.p);
+    count_launch();
+    FHS_LAUNCH_CHECK();
   }
 }
 
@@ -295,18 +432,17 @@ __global__ void crop_real_kernel(const float2* __restrict__ grid, float* __restr
   }
 }
 
-__global__ void block_reduce_kernel(const double* __restrict__ partials, int ntiles, int c0,
+__global__ void block_reduce_kernel(const double* __restrict__ partials, const int* __restrict__ slot_off, int c0,
                                     const int32_t* __restrict__ ch_nblk, const int32_t* __restrict__ ch_blkoff,
                                     const double* __restrict__ blk_eps, float* __restrict__ blk_scale,
                                     double* __restrict__ blk_stats) {
-  const int c = blockIdx.x;  // relative channel
-  const int ch = c0 + c;
+  const int ch = c0 + blockIdx.x;
   const int b = blockIdx.y;
   if (b >= ch_nblk[ch]) return;
   __shared__ double s0[256], s1[256];
   double a = 0, r = 0;
-  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) {
-    const double* pp = partials + ((size_t)c * ntiles + t) * kMaxBlocksPerChannel * 2;
+  for (int t = slot_off[ch] + threadIdx.x; t < slot_off[ch + 1]; t += blockDim.x) {
+    const double* pp = partials + (size_t)t * kMaxBlocksPerChannel * 2;
     a += pp[2 * b];
     r += pp[2 * b + 1];
   }
@@ -481,6 +617,76 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
   h.set = true;
 }
 
+// Work lists for the tile kernels.  Degridding: one item per non-empty
+// (channel, tile), split into slices of at most kDegridSlice visibilities.
+// Gridding: one item per (channel, tile) whose footprint ring holds any
+// visibility, split into slices of at most kGridSlice; split tiles get partial
+// tiles that grid_combine_kernel sums.  Empty tiles are never written (the
+// gridding output is zeroed at commit).  Items run channel by channel in tile
+// order, so neighbouring tiles (which share aprons) run close together.
+constexpr int kDegridSlice = 8192;
+constexpr int kGridSlice = 4096;
+
+static void build_work_lists(MeasOp* op, cudaStream_t s) {
+  const int L = op->L, nt = op->ntiles();
+  const int S = kSubPerTile;
+  auto key = [&](int sb0, int sb1) {
+    return ((sb1 / S) * op->nT0 + sb0 / S) * (S * S) + (sb1 % S) * S + (sb0 % S);
+  };
+  std::vector<WorkItem> dg, gr;
+  std::vector<GridCombine> comb;
+  op->h_dg_off.assign(L + 1, 0);
+  op->h_gr_off.assign(L + 1, 0);
+  op->h_comb_off.assign(L + 1, 0);
+  int pslot = 0;
+  for (int c = 0; c < L; ++c) {
+    const std::vector<int32_t>& off = op->ch[c].sb_off;
+    for (int t = 0; t < nt; ++t) {
+      const int t0 = t % op->nT0, t1 = t / op->nT0;
+      const int own = off[(t + 1) * S * S] - off[t * S * S];
+      if (own > 0) {
+        const int ns = (own + kDegridSlice - 1) / kDegridSlice;
+        for (int k = 0; k < ns; ++k) {
+          dg.push_back(WorkItem{c, t, k, ns, (int)dg.size(), 0});
+        }
+      }
+      // visibilities starting in the tile or in the 8-cell ring left/above it
+      int ring = 0;
+      const int sbc1 = (t1 * S - 1 + op->nsb1) % op->nsb1, sbr0 = (t0 * S - 1 + op->nsb0) % op->nsb0;
+      const int r_end = std::min(t0 * S + S, op->nsb0), c_end = std::min(t1 * S + S, op->nsb1);
+      for (int sb0 = t0 * S; sb0 < r_end; ++sb0) ring += off[key(sb0, sbc1) + 1] - off[key(sb0, sbc1)];
+      for (int sb1 = t1 * S; sb1 < c_end; ++sb1) ring += off[key(sbr0, sb1) + 1] - off[key(sbr0, sb1)];
+      ring += off[key(sbr0, sbc1) + 1] - off[key(sbr0, sbc1)];
+      const int tot = own + ring;
+      if (tot == 0) continue;
+      const int ns = (tot + kGridSlice - 1) / kGridSlice;
+      if (ns == 1) {
+        gr.push_back(WorkItem{c, t, 0, 1, -1, 0});
+      } else {
+        comb.push_back(GridCombine{c, t, pslot, ns});
+        for (int k = 0; k < ns; ++k) {
+          gr.push_back(WorkItem{c, t, k, ns, pslot + k, 0});
+        }
+        pslot += ns;
+      }
+    }
+    op->h_dg_off[c + 1] = (int)dg.size();
+    op->h_gr_off[c + 1] = (int)gr.size();
+    op->h_comb_off[c + 1] = (int)comb.size();
+  }
+  op->dg_items.alloc(std::max<size_t>(dg.size(), 1));
+  op->dg_items.upload(dg.data(), dg.size(), s);
+  op->gr_items.alloc(std::max<size_t>(gr.size(), 1));
+  op->gr_items.upload(gr.data(), gr.size(), s);
+  op->gr_combine.alloc(std::max<size_t>(comb.size(), 1));
+  op->gr_combine.upload(comb.data(), comb.size(), s);
+  op->dg_off.alloc(L + 1);
+  op->dg_off.upload(op->h_dg_off.data(), L + 1, s);
+  op->gr_partial.alloc(std::max<size_t>((size_t)pslot * kTileCells * kTileCells, 1));
+  op->partials.alloc(std::max<size_t>(dg.size(), 1) * kMaxBlocksPerChannel * 2);
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
 void measop_commit(MeasOp* op) {
   FHS_CHECK(!op->committed, FHS_ERR_STATE, "operator already committed");
   for (int c = 0; c < op->L; ++c) FHS_CHECK(op->ch[c].set, FHS_ERR_STATE, "channel " + std::to_string(c) + " not set");
@@ -546,7 +752,7 @@ void measop_commit(MeasOp* op) {
   op->gridA.alloc(gsz);
   op->gridB.alloc(gsz);
   op->gridB.zero(s);
-  op->partials.alloc((size_t)L * op->ntiles() * kMaxBlocksPerChannel * 2);
+  build_work_lists(op, s);
   op->blk_stats.alloc((size_t)std::max(op->nblk_tot, 1) * 2);
   op->blk_scale.alloc((size_t)L * kMaxBlocksPerChannel);
   op->blk_scale.zero(s);
@@ -594,18 +800,16 @@ void fft_inverse(const MeasOp* op, int p0, int np, cudaStream_t s) {
 }
 
 void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s) {
-  dim3 grid(op->ntiles(), nc);
-  degrid_kernel<7, false><<<grid, 256, 0, s>>>(op->view(), op->gridA.p, c0, out, nullptr, nullptr, nullptr,
-                                               nullptr, nullptr);
+  const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
+  if (n == 0) return;
+  degrid_kernel<7, false><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr,
+                                            i0, out, nullptr, nullptr, nullptr, nullptr, nullptr);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
 
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s) {
-  dim3 grid(op->ntiles(), nc);
-  grid_kernel<7, false><<<grid, 256, 0, s>>>(op->view(), op->gridB.p, c0, v, nullptr, nullptr, nullptr);
-  count_launch();
-  FHS_LAUNCH_CHECK();
+  launch_grid_kernel<7, false>(op, c0, nc, v, nullptr, nullptr, nullptr, s);
 }
 
 void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s) {
@@ -618,27 +822,24 @@ void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, 
 
 void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
                         cudaStream_t s) {
-  dim3 grid(op->ntiles(), nc);
-  degrid_kernel<7, true><<<grid, 256, 0, s>>>(op->view(), op->gridA.p, c0, nullptr, v2, gold, y,
-                                              op->partials.p, op->zbuf.p);
+  const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
+  if (n == 0) return;
+  degrid_kernel<7, true><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr,
+                                           i0, nullptr, v2, gold, y, op->partials.p, op->zbuf.p);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
 
 void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s) {
   dim3 grid(nc, kMaxBlocksPerChannel);
-  block_reduce_kernel<<<grid, 256, 0, s>>>(op->partials.p, op->ntiles(), c0, op->ch_nblk.p, op->ch_blkoff.p,
+  block_reduce_kernel<<<grid, 256, 0, s>>>(op->partials.p, op->dg_off.p, c0, op->ch_nblk.p, op->ch_blkoff.p,
                                            op->blk_eps.p, op->blk_scale.p, op->blk_stats.p);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
 
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s) {
-  dim3 grid(op->ntiles(), nc);
-  grid_kernel<7, true><<<grid, 256, 0, s>>>(op->view(), op->gridB.p, c0, nullptr, v2, op->blk_scale.p,
-                                            op->zbuf.p);
-  count_launch();
-  FHS_LAUNCH_CHECK();
+  launch_grid_kernel<7, true>(op, c0, nc, nullptr, v2, op->blk_scale.p, op->zbuf.p, s);
 }
 
 }  // namespace fhs

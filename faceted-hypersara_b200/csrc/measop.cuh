@@ -25,6 +25,20 @@ struct OpView {
   const int32_t* ch_M;    // [L]
 };
 
+// A slice of one (channel, tile) for the degridding / gridding kernels.
+// Dense tiles are split so that no CTA carries more than a fixed number of
+// visibilities (the uv coverage is strongly concentrated near the origin).
+struct WorkItem {
+  int ch, tile;
+  int split, nsplit;
+  int slot;   // degrid: block-norm partial slot; grid: partial tile slot (-1: write the grid)
+  int pad;
+};
+
+struct GridCombine {
+  int ch, tile, pbase, nsplit;
+};
+
 struct ChannelHost {
   std::vector<float4> geom;        // sorted order
   std::vector<int32_t> perm;       // sorted position -> original index
@@ -70,7 +84,14 @@ struct MeasOp {
   DevBuf<float2> vis_a, vis_b;
   DevBuf<double> stage;     // host-format staging (double)
   DevBuf<float> img_a;      // [L][N] image scratch
-  DevBuf<double> partials;  // [L][ntiles][kMaxBlocksPerChannel][2]
+  DevBuf<double> partials;  // [degrid items][kMaxBlocksPerChannel][2]
+  // work lists: channel-major items (+ per-channel offsets)
+  DevBuf<WorkItem> dg_items, gr_items;
+  std::vector<int> h_dg_off, h_gr_off;   // [L+1] item offsets per channel
+  DevBuf<int> dg_off;                    // device copy of h_dg_off
+  DevBuf<GridCombine> gr_combine;
+  std::vector<int> h_comb_off;           // [L+1] combine entries per channel
+  DevBuf<float2> gr_partial;             // [partial slots][tile cells]
   DevBuf<double> blk_stats; // [nblk_tot][2]: ||z||^2, ||res||^2
   DevBuf<float> blk_scale;  // [L][kMaxBlocksPerChannel]
   DevBuf<double> blk_eps;   // [L][kMaxBlocksPerChannel]
