@@ -121,13 +121,19 @@ def _init_pg(world, local):
     return dist
 
 
-def _max_over_ranks(dist, value, local):
+def _max_over_ranks(dist, value, device):
+    """Max of a per-rank scalar over all ranks (device: 'cuda:i' for NCCL, 'cpu' for gloo)."""
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_value(world, steps, ms_max):
+    """Whole-job throughput: every rank runs `steps` iterations of its own cube."""
+    return world * steps / (ms_max / 1e3)
 
 
 def _barrier(dist, local):
@@ -264,8 +270,8 @@ def run_ours(args):
     launches = lib().fhs_kernel_launch_count() - l0
     _barrier(dist, local)
     clocks = sampler.stop()
-    ms_max = _max_over_ranks(dist, ms, local)
-    value = world * args.steps / (ms_max / 1e3)
+    ms_max = _max_over_ranks(dist, ms, f"cuda:{local}")
+    value = aggregate_value(world, args.steps, ms_max)
     # ---- per-stage device times (same stream, stage-by-stage launches)
     stages = s.profile_stages(3)
     from fhs_b200 import sara_n_coefs
@@ -286,7 +292,7 @@ def run_ours(args):
         e2e = _e2e(prob, s, args.steps)
     except Exception as e:  # reported, not hidden
         e2e = {"error": str(e)}
-    e2e_v = _max_over_ranks(dist, e2e.get("seconds", 0.0), local) if "seconds" in e2e else None
+    e2e_v = _max_over_ranks(dist, e2e.get("seconds", 0.0), f"cuda:{local}") if "seconds" in e2e else None
     if e2e_v:
         e2e = {"value": world * args.steps / e2e_v, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"],
                "d2h_bytes_per_step": e2e["d2h"],

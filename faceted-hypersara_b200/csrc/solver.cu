@@ -130,42 +130,54 @@ __global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, float* __
   }
 }
 
-__global__ void stats_kernel(const double* __restrict__ primal_part, int nparts, int lg, int G,
-                             const double* __restrict__ blk_stats, const int32_t* __restrict__ ch_nblk,
-                             const int32_t* __restrict__ ch_blkoff, const double* __restrict__ blk_eps,
-                             const double* __restrict__ nuc_vals, int Q, const double* __restrict__ l21_part,
-                             int prox_blocks, const double* __restrict__ l21_acc, double* __restrict__ ring,
-                             int* __restrict__ counter) {
-  __shared__ int c;
-  if (threadIdx.x == 0) c = *counter;
-  __syncthreads();
-  double* rec = ring + (size_t)(c % kReportRing) * G * kReportFields;
-  for (int g = threadIdx.x; g < G; g += blockDim.x) {
-    double rx = 0, nx = 0, r2 = 0, e2 = 0, nu = 0, l21 = 0;
-    for (int l = g * lg; l < (g + 1) * lg; ++l) {
-      for (int k = 0; k < nparts; ++k) {
-        rx += primal_part[((size_t)l * nparts + k) * 2];
-        nx += primal_part[((size_t)l * nparts + k) * 2 + 1];
-      }
-      for (int b = 0; b < ch_nblk[l]; ++b) {
-        r2 += blk_stats[2 * (ch_blkoff[l] + b) + 1];
-        const double e = blk_eps[(size_t)l * kMaxBlocksPerChannel + b];
-        e2 += e * e;
-      }
-    }
-    if (nuc_vals)
-      for (int q = 0; q < Q; ++q) nu += nuc_vals[g * Q + q];
-    for (int k = 0; k < prox_blocks; ++k) l21 += l21_part[(size_t)g * prox_blocks + k];
-    l21 += l21_acc[g];
-    rec[g * kReportFields + 0] = rx;
-    rec[g * kReportFields + 1] = nx;
-    rec[g * kReportFields + 2] = r2;
-    rec[g * kReportFields + 3] = e2;
-    rec[g * kReportFields + 4] = nu;
-    rec[g * kReportFields + 5] = l21;
+// One CTA per spectral group reduces the iteration's FP64 statistics into the
+// device ring; the last CTA to finish advances the ring counter.
+__global__ void __launch_bounds__(256) stats_kernel(const double* __restrict__ primal_part, int nparts, int lg, int G,
+                                                    const double* __restrict__ blk_stats,
+                                                    const int32_t* __restrict__ ch_nblk,
+                                                    const int32_t* __restrict__ ch_blkoff,
+                                                    const double* __restrict__ blk_eps,
+                                                    const double* __restrict__ nuc_vals, int Q,
+                                                    const double* __restrict__ l21_part, int prox_blocks,
+                                                    const double* __restrict__ l21_acc, double* __restrict__ ring,
+                                                    int* __restrict__ counter, int* __restrict__ done) {
+  __shared__ double red[6][256];
+  __shared__ int last;
+  const int g = blockIdx.x;
+  const int c = *counter;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = threadIdx.x; k < lg * nparts; k += blockDim.x) {
+    const int l = g * lg + k / nparts, kk = k % nparts;
+    v[0] += primal_part[((size_t)l * nparts + kk) * 2];
+    v[1] += primal_part[((size_t)l * nparts + kk) * 2 + 1];
   }
+  for (int l = g * lg + threadIdx.x; l < (g + 1) * lg; l += blockDim.x)
+    for (int b = 0; b < ch_nblk[l]; ++b) {
+      v[2] += blk_stats[2 * (ch_blkoff[l] + b) + 1];
+      const double e = blk_eps[(size_t)l * kMaxBlocksPerChannel + b];
+      v[3] += e * e;
+    }
+  if (nuc_vals)
+    for (int q = threadIdx.x; q < Q; q += blockDim.x) v[4] += nuc_vals[g * Q + q];
+  for (int k = threadIdx.x; k < prox_blocks; k += blockDim.x) v[5] += l21_part[(size_t)g * prox_blocks + k];
+  if (threadIdx.x == 0) v[5] += l21_acc[g];
+  for (int f = 0; f < 6; ++f) red[f][threadIdx.x] = v[f];
   __syncthreads();
-  if (threadIdx.x == 0) *counter = c + 1;
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int f = 0; f < 6; ++f) red[f][threadIdx.x] += red[f][threadIdx.x + s];
+    __syncthreads();
+  }
+  double* rec = ring + (size_t)(c % kReportRing) * G * kReportFields;
+  if (threadIdx.x < 6) rec[g * kReportFields + threadIdx.x] = red[threadIdx.x][0];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(done, 1) == G - 1);
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    *done = 0;
+    *counter = c + 1;
+  }
 }
 
 __global__ void weights_kernel(const float* __restrict__ norms, int64_t s, const double* __restrict__ ups,
@@ -279,11 +291,11 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   count_launch();
   FHS_LAUNCH_CHECK();
   mark();
-  stats_kernel<<<1, 64, 0, s>>>(S->primal_part.p, kPrimalBlocks, S->lg, S->G, op->blk_stats.p, op->ch_nblk.p,
+  stats_kernel<<<S->G, 256, 0, s>>>(S->primal_part.p, kPrimalBlocks, S->lg, S->G, op->blk_stats.p, op->ch_nblk.p,
                                 op->ch_blkoff.p, op->blk_eps.p, S->nuclear ? S->nuc_vals.p : nullptr,
                                 S->nuclear ? S->np.Q : 0, S->l21_part.p,
                                 sara_fused_supported(S->lg) ? 0 : S->prox_blocks, S->l21_acc.p, S->ring.p,
-                                S->ring_counter.p);
+                                S->ring_counter.p, S->ring_counter.p + 1);
   count_launch();
   FHS_LAUNCH_CHECK();
   mark();
@@ -438,7 +450,8 @@ fhs_status fhs_solver_create(fhs_measop* op_, const fhs_solver_config* cfg, fhs_
     S->l21_acc.alloc(S->G);
     S->l21_acc.zero(s);
     S->ring.alloc((size_t)kReportRing * S->G * kReportFields);
-    S->ring_counter.alloc(1);
+    S->ring_counter.alloc(2);  // [0] iterations recorded, [1] CTAs done in the current one
+    S->ring_counter.zero(s);
     FHS_CUDA(cudaStreamSynchronize(s));
     *out = reinterpret_cast<fhs_solver*>(S.release());
   });

@@ -99,3 +99,27 @@ def test_final_snr_matches_oracle(algo):
     snr_g, snr_o = so.snr_db(x, xg), so.snr_db(x, xo)
     assert abs(snr_g - snr_o) < SNR_TOL_DB, (snr_g, snr_o, info, log.n_iter)
     assert snr_o > 15.0
+
+
+def test_fhs_iterations_match_golden_fixture():
+    """Three GPU FHS iterations against the committed FP64 fixture."""
+    import os
+
+    from fhs_b200 import MeasurementOperator, Solver
+    from fhs_b200._lib import ALGO_FHS
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fhs_24x24x2_3iter.npz"))
+    om = [(g["om_y0"], g["om_x0"]), (g["om_y1"], g["om_x1"])]
+    blocks = [list(b) for b in g["blocks"]]
+    op = MeasurementOperator(24, 24, om, blocks, [np.full(len(o[0]), 1.0 / s) for o, s in zip(om, g["sigma"])])
+    y = [op.split(0, g["y0"]), op.split(1, g["y1"])]
+    eps = [synth.l2_bounds(b) for b in blocks]
+    param = dict(nu2=g["nu2"], gamma=float(g["sig"]), gamma0=g["sig_bar"], reweighting_sig=float(g["sig"]),
+                 reweighting_sig_bar=g["sig_bar"], pdfb_min_iter=10 ** 6, reweighting_flag=False)
+    geom = FacetGeometry(24, 24, 2, 2, (3, 3))
+    s = Solver(op, ALGO_FHS, param, Qy=2, Qx=2, overlap=(3, 3),
+               splits_y=[r[0] for r in geom.base_y] + [24], splits_x=[r[0] for r in geom.base_x] + [24])
+    s.set_data(y, eps)
+    s.init()
+    s.iterate(3)
+    assert rel(np.moveaxis(s.x(), 2, 0), g["x3"]) < ITER_TOL
+    s.close()
