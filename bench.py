@@ -30,8 +30,10 @@ METRIC = "FHS 1024²×64 iter/s & time-to-converge: warm-start vs plain, 1×B200
 UNIT = "iter/s"
 WORKLOAD = dict(Ny=1024, Nx=1024, L=64, C=4, Q=4, overlap_frac=0.1, jitter=0.15, m_lo=0.3, m_hi=1.0,
                 blocks=(2, 6), snr_db=40.0)
-# reduced case for ncu captures (same kernels, ~0.6 GB of grids)
+# reduced cases for ncu captures: small (~0.6 GB of grids) and medium (the
+# bench's kernel instantiations, 16 channels per sub-cube, ~2 GB of grids)
 SMALL = dict(WORKLOAD, Ny=512, Nx=512, L=16)
+MEDIUM = dict(WORKLOAD, Ny=512, Nx=512, L=64)
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -255,7 +257,7 @@ def run_ours(args):
     from fhs_b200 import lib
     from fhs_b200.workload import build_problem, make_solver
     seed = 1000 + rank
-    wl = SMALL if args.case == "small" else WORKLOAD
+    wl = {"small": SMALL, "medium": MEDIUM}.get(args.case, WORKLOAD)
     prob = build_problem(**wl, seed=seed, device=local)
     s = make_solver(prob)
     s.init()
@@ -309,7 +311,7 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": _config({"visibilities": prob["n_vis"], "parallelism": f"{world} independent cubes"})
-                if args.case == "full" else {"workload": "fhs_512x512x16_C4_Q4x4 (profiling case)"},
+                if args.case == "full" else {"workload": f"fhs_{wl['Ny']}x{wl['Nx']}x{wl['L']}_C4_Q4x4 (profiling case)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks, "stages_ms": stage_rows,
                 "vis_per_s": 2.0 * prob["n_vis"] * value}
@@ -351,8 +353,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["full", "small"], default="full",
-                    help="small: 512x512x16 profiling case for ncu captures (not a bench line)")
+    ap.add_argument("--case", choices=["full", "medium", "small"], default="full",
+                    help="medium (512x512x64) / small (512x512x16): profiling cases for ncu captures, not bench lines")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
