@@ -123,7 +123,63 @@ __global__ void plane_scale_kernel(float* __restrict__ x, int64_t N, const doubl
     x[(size_t)p * N + i] *= s;
 }
 
+__global__ void vis_axpy_kernel(float2* __restrict__ y, const float2* __restrict__ x, float a, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 v = x[i];
+    y[i] = make_float2(fmaf(a, v.x, y[i].x), fmaf(a, v.y, y[i].y));
+  }
+}
+
+__global__ void plane_set_kernel(float* __restrict__ x, int64_t N, int np, int64_t idx, float v) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < np) x[(size_t)p * N + idx] = v;
+}
+
+__global__ void plane_max_kernel(const float* __restrict__ x, int64_t N, double* __restrict__ out) {
+  __shared__ float sh[1024];
+  const int p = blockIdx.x;
+  float m = -INFINITY;
+  for (int64_t i = threadIdx.x; i < N; i += blockDim.x) m = fmaxf(m, x[(size_t)p * N + i]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + k]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[p] = sh[0];
+}
+
+__global__ void plane_scale_inv_kernel(float* __restrict__ x, int64_t N, const double* __restrict__ f) {
+  const int p = blockIdx.y;
+  const float s = (float)(1.0 / f[p]);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+    x[(size_t)p * N + i] *= s;
+}
+
 }  // namespace
+
+void launch_vis_axpy(float2* y, const float2* x, float a, int64_t n, cudaStream_t s) {
+  if (n <= 0) return;
+  vis_axpy_kernel<<<nblk(n), 256, 0, s>>>(y, x, a, n);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+void launch_plane_set(float* x, int64_t N, int np, int64_t idx, float v, cudaStream_t s) {
+  plane_set_kernel<<<(np + 255) / 256, 256, 0, s>>>(x, N, np, idx, v);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+void launch_plane_max(const float* x, int64_t N, int np, double* out, cudaStream_t s) {
+  plane_max_kernel<<<np, 1024, 0, s>>>(x, N, out);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+void launch_plane_scale_inv(float* x, int64_t N, int np, const double* f, cudaStream_t s) {
+  dim3 grid(nblk(N), np);
+  plane_scale_inv_kernel<<<grid, 256, 0, s>>>(x, N, f);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
 
 void launch_d2f(const double* in, float* out, int64_t n, cudaStream_t s) {
   if (n <= 0) return;

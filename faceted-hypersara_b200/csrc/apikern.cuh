@@ -27,6 +27,14 @@ void launch_crop_complex(const float2* grid, double* out, const float* sy, const
                          int Ky, int Kx, int np, cudaStream_t s);
 // per-plane sum of squares (FP64): out[p] = sum x[p][:]^2
 void launch_plane_sumsq(const float* x, int64_t N, int np, double* out, cudaStream_t s);
+// y <- y + a * x (float2 vectors of length n)
+void launch_vis_axpy(float2* y, const float2* x, float a, int64_t n, cudaStream_t s);
+// x[p][idx] = v for every plane
+void launch_plane_set(float* x, int64_t N, int np, int64_t idx, float v, cudaStream_t s);
+// out[p] = max x[p][:] (FP64)
+void launch_plane_max(const float* x, int64_t N, int np, double* out, cudaStream_t s);
+// x[p][:] /= f[p]
+void launch_plane_scale_inv(float* x, int64_t N, int np, const double* f, cudaStream_t s);
 // per-plane scale: x[p][:] *= f[p]
 void launch_plane_scale(float* x, int64_t N, int np, const double* f, cudaStream_t s);
 

@@ -218,6 +218,51 @@ fhs_status fhs_adjoint_operator(fhs_measop* op_, const double* y, double* x) {
   });
 }
 
+fhs_status fhs_compute_residual_images(fhs_measop* op_, const double* y, const double* x, double* res) {
+  return guarded([&] {
+    MeasOp* op = committed(op_);
+    FHS_CHECK(y && x && res, FHS_ERR_INVALID_ARG, "null buffer");
+    DeviceGuard g(op->device);
+    cudaStream_t s = op->stream;
+    const int64_t N = op->Npix();
+    const int L = op->L;
+    double* st = stage(op, std::max<int64_t>(N * L, 2 * op->Mtot));
+    float* img = img_scratch(op);
+    float2* va = vis_scratch(op, op->vis_a);
+    float2* vb = vis_scratch(op, op->vis_b);
+    DevBuf<float> psf;
+    psf.alloc((size_t)N * L);
+    DevBuf<double> peak;
+    peak.alloc(L);
+    // residual visibilities y - G A x
+    FHS_CUDA(cudaMemcpyAsync(st, y, 2 * op->Mtot * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_vis_gather(st, vb, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
+    FHS_CUDA(cudaMemcpyAsync(st, x, N * L * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_d2f(st, img, N * L, s);
+    launch_pad(op, img, 0, L, s);
+    fft_forward(op, 0, L, s);
+    launch_degrid_plain(op, 0, L, va, s);
+    launch_vis_axpy(vb, va, -1.f, op->Mtot, s);  // vb <- y - G A x
+    launch_grid_plain(op, 0, L, vb, s);
+    fft_inverse(op, 0, L, s);
+    launch_crop_real(op, img, nullptr, 0, L, s);
+    // PSF: a dirac at (N/2, N/2) (0-based) through G^H G A
+    FHS_CUDA(cudaMemsetAsync(psf.p, 0, (size_t)N * L * sizeof(float), s));
+    launch_plane_set(psf.p, N, L, (int64_t)(op->Nx / 2) * op->Ny + op->Ny / 2, 1.f, s);
+    launch_pad(op, psf.p, 0, L, s);
+    fft_forward(op, 0, L, s);
+    launch_degrid_plain(op, 0, L, va, s);
+    launch_grid_plain(op, 0, L, va, s);
+    fft_inverse(op, 0, L, s);
+    launch_crop_real(op, psf.p, nullptr, 0, L, s);
+    launch_plane_max(psf.p, N, L, peak.p, s);
+    launch_plane_scale_inv(img, N, L, peak.p, s);
+    launch_f2d(img, st, N * L, s);
+    FHS_CUDA(cudaMemcpyAsync(res, st, N * L * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FHS_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 fhs_status fhs_operator_norm(fhs_measop* op_, int max_iter, double tol, double* sq) {
   return guarded([&] {
     MeasOp* op = committed(op_);

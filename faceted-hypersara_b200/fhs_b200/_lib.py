@@ -78,6 +78,7 @@ SIGNATURES = {
     "fhs_forward_operator": (C.c_int, [_vp, _dp, _dp]),
     "fhs_adjoint_operator": (C.c_int, [_vp, _dp, _dp]),
     "fhs_operator_norm": (C.c_int, [_vp, C.c_int, C.c_double, _dp]),
+    "fhs_compute_residual_images": (C.c_int, [_vp, _dp, _dp, _dp]),
     "fhs_update_dual_data_fidelity": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "fhs_proj_l2ball": (C.c_int, [C.c_int, C.c_int64, _dp, C.c_double, _dp, _dp]),
     "fhs_proj_l2ball_noalloc": (C.c_int, [C.c_int, C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,

@@ -164,6 +164,16 @@ def HS_adjoint_operator_G(y, op: MeasurementOperator):
     return x.reshape(op.Ny, op.Nx, op.L, order="F")
 
 
+def compute_residual_images(x, y, op: MeasurementOperator):
+    """src/compute_residual_images.m:83-102 (no DR): PSF-normalised residual
+    images real(At(G'(y - G A x))) -> [Ny, Nx, L]."""
+    xc = _cube_in(x, op.Ny, op.Nx)
+    yf = _cplx_in(np.concatenate([op.flatten(v) for v in y]))
+    out = np.empty(op.Ny * op.Nx * op.L)
+    check(lib().fhs_compute_residual_images(op.handle, dptr(yf), dptr(xc.reshape(-1, order="F")), dptr(out)))
+    return out.reshape(op.Ny, op.Nx, op.L, order="F")
+
+
 def proj_l2ball(x, eps, y, device: int = 0):
     """src/proj_l2ball.m:20-22 on the GPU (FP64)."""
     x = np.asarray(x)

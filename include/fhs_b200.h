@@ -92,6 +92,10 @@ FHS_API fhs_status fhs_apply_adjoint_operator(fhs_measop* op, int channel, const
 FHS_API fhs_status fhs_forward_operator(fhs_measop* op, const double* x, double* y);
 /* lib/operators/HS_adjoint_operator_G.m:42-57 followed by real(): y -> x[Ny,Nx,L]. */
 FHS_API fhs_status fhs_adjoint_operator(fhs_measop* op, const double* y, double* x);
+/* src/compute_residual_images.m:83-102 (no DR): res[Ny,Nx,L] =
+ * real(At(G'(y - G A x))) per channel, divided by the peak of the PSF
+ * real(At(G'G A dirac)) with the dirac at pixel (Ny/2+1, Nx/2+1) (1-based). */
+FHS_API fhs_status fhs_compute_residual_images(fhs_measop* op, const double* y, const double* x, double* res);
 /* lib/utils/util_operator_norm.m:43-61: per-channel ||G_l A||^2 by power
  * iteration (op_norm of the submodule), FP32 operators, FP64 norms. */
 FHS_API fhs_status fhs_operator_norm(fhs_measop* op, int max_iter, double tol, double* squared_norms);

@@ -84,6 +84,75 @@ def adjoint_operator(yb, data: DataTerm):
     return out
 
 
+def uniform_weight_preconditioner(om_y, om_x, Ky, Kx):
+    """Uniform-weighting preconditioner (util_gen_preconditioning_matrix of the
+    missing submodule, gen_uniform_weight_matrix = true, one sub-pixel, as set
+    in imaging/default_parameters.json "preconditioning"): pU = 1 / (number
+    of visibilities falling in the same cell of the Ky x Kx Fourier grid),
+    cells centred on the grid points."""
+    ky = np.mod(np.floor(np.asarray(om_y) * Ky / (2 * np.pi) + 0.5), Ky).astype(np.int64)
+    kx = np.mod(np.floor(np.asarray(om_x) * Kx / (2 * np.pi) + 0.5), Kx).astype(np.int64)
+    cell = ky + Ky * kx
+    cnt = np.bincount(cell, minlength=Ky * Kx)
+    return 1.0 / cnt[cell]
+
+
+def proj_ellipse_fb(s, y, pU, eps, z0, max_itr=20, min_itr=1, stop=1e-8):
+    """Projection onto {||z - y|| <= eps} in the metric diag(1/pU):
+    argmin_z (z-s)^H diag(1/pU) (z-s)/2 with ||z - y|| <= eps, by
+    forward-backward iterations z <- P_B(z - mu (z - s)/pU), mu = min(pU)
+    (Onose et al. 2017; solver_proj_elipse_fb of the missing submodule,
+    called at src/update_dual_data_fidelity.m:133-135 and src/sara/sara.m:594).
+    With pU = 1 one iteration is the exact l2-ball projection of s."""
+    mu = float(np.min(pU))
+    z = np.array(z0, dtype=np.complex128)
+    k = 0
+    for k in range(1, max_itr + 1):
+        t = z - mu * (z - s) / pU
+        zn = proj_l2ball(t, eps, y)
+        dz = np.linalg.norm(zn - z)
+        nz = np.linalg.norm(zn)
+        z = zn
+        if k >= min_itr and dz <= stop * nz:
+            break
+    return z, k
+
+
+def update_dual_data_fidelity_precond(v2, proj, x, Fx_old, data: DataTerm, pU, sigma22, max_itr=20, min_itr=1,
+                                      stop=1e-8):
+    """src/update_dual_data_fidelity.m:126-147 with a preconditioner pU[l][b]:
+    proj = solver_proj_elipse_fb(v2/pU, r2, y, pU, eps, proj, ...),
+    v2 = v2 + pU (r2 - proj).  Returns (v2, proj, Ftx, Fx_old, norm_res,
+    global_norm_res^2, norm_epsilon^2)."""
+    op = data.op
+    Ftx = np.zeros_like(x)
+    norm_res, v2n, pn = [], [], []
+    gres, geps = 0.0, 0.0
+    Fx_new = np.empty_like(Fx_old)
+    for l in range(data.L):
+        Fx = op.A(x[l])
+        g2 = np.zeros(op.No, dtype=np.complex128)
+        nr, vl, pl = [], [], []
+        for b, G in enumerate(data.G[l]):
+            r2 = G @ (2.0 * Fx - Fx_old[l])
+            s = v2[l][b] / pU[l][b] + r2
+            p, _ = proj_ellipse_fb(s, data.y[l][b], pU[l][b], data.eps[l][b], proj[l][b], max_itr, min_itr, stop)
+            vb = v2[l][b] + pU[l][b] * (r2 - p)
+            vl.append(vb)
+            pl.append(p)
+            g2 += G.conj().T @ vb
+            res = np.linalg.norm(G @ Fx - data.y[l][b])
+            nr.append(res)
+            gres += res ** 2
+            geps += data.eps[l][b] ** 2
+        v2n.append(vl)
+        pn.append(pl)
+        norm_res.append(nr)
+        Fx_new[l] = Fx
+        Ftx[l] = sigma22[l] * np.real(op.At(g2))
+    return v2n, pn, Ftx, Fx_new, norm_res, gres, geps
+
+
 def update_dual_data_fidelity(v2, x, Fx_old, data: DataTerm, sigma22):
     """src/update_dual_data_fidelity.m:116-147 with pU = 1.
 
@@ -114,6 +183,28 @@ def update_dual_data_fidelity(v2, x, Fx_old, data: DataTerm, sigma22):
         Fx_new[l] = Fx
         Ftx[l] = sigma22[l] * np.real(op.At(g2))
     return v2n, Ftx, Fx_new, norm_res, gres, geps
+
+
+def compute_residual_images(x, data: DataTerm):
+    """src/compute_residual_images.m:83-102 (no DR): real(At(G'(y - G A x)))
+    per channel, normalised by the peak of the PSF real(At(G'G A dirac)),
+    dirac at pixel (N/2+1, N/2+1) (1-based)."""
+    op = data.op
+    out = np.zeros_like(x)
+    dirac = np.zeros((op.Ny, op.Nx))
+    dirac[op.Ny // 2, op.Nx // 2] = 1.0
+    for l in range(data.L):
+        Fx = op.A(x[l])
+        r = np.zeros(op.No, dtype=np.complex128)
+        for G, yb in zip(data.G[l], data.y[l]):
+            r += G.conj().T @ (yb - G @ Fx)
+        res = np.real(op.At(r))
+        Fd = op.A(dirac)
+        rp = np.zeros(op.No, dtype=np.complex128)
+        for G in data.G[l]:
+            rp += G.conj().T @ (G @ Fd)
+        out[l] = res / np.max(np.real(op.At(rp)))
+    return out
 
 
 def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0):

@@ -82,3 +82,17 @@ def test_operator_norm_matches_oracle():
     nu_gpu = gop.operator_norm(200, 1e-8)
     nu_ref = operator_norm(DataTerm(ref, [[G] for G in Gs], [[None]] * 2, [[1.0]] * 2), 200, 1e-10)
     assert np.allclose(nu_gpu, nu_ref, rtol=1e-4)
+
+
+def test_compute_residual_images_matches_oracle():
+    from fhs_b200 import compute_residual_images, synth
+    from oracle import problem
+    from oracle import solvers as so
+    data, x, meta = problem.make_problem(48, 40, 3, 2000, 2, seed=13, synth=synth)
+    from fhs_b200 import MeasurementOperator
+    op = MeasurementOperator(48, 40, meta["om"], meta["blocks"],
+                             [np.full(len(o[0]), 1.0 / s) for o, s in zip(meta["om"], meta["sigma"])])
+    xk = 0.8 * x
+    res = compute_residual_images(np.moveaxis(xk, 0, 2), data.y, op)
+    ref = so.compute_residual_images(xk, data)
+    assert rel(np.moveaxis(res, 2, 0), ref) < OP_TOL * 10
