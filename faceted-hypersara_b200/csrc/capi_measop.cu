@@ -57,6 +57,107 @@ static float* img_scratch(MeasOp* op) {
   return op->img_a.p;
 }
 
+// HS_forward_operator_G.m:36-52 (precond: HS_forward_operator_precond_G.m:40-55,
+// y = sqrt(pU) .* G A x), all channels, host buffers.
+static void forward_impl(MeasOp* op, const double* x, double* y, bool precond) {
+  FHS_CHECK(x && y, FHS_ERR_INVALID_ARG, "null buffer");
+  FHS_CHECK(!precond || op->precond, FHS_ERR_STATE, "no preconditioner set");
+  DeviceGuard g(op->device);
+  cudaStream_t s = op->stream;
+  const int64_t N = op->Npix();
+  double* st = stage(op, std::max<int64_t>(N * op->L, 2 * op->Mtot));
+  float* img = img_scratch(op);
+  float2* va = vis_scratch(op, op->vis_a);
+  FHS_CUDA(cudaMemcpyAsync(st, x, N * op->L * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_d2f(st, img, N * op->L, s);
+  launch_pad(op, img, 0, op->L, s);
+  fft_forward(op, 0, op->L, s);
+  launch_degrid_plain(op, 0, op->L, va, s);
+  if (precond) launch_scale_pu(op, va, true, s);
+  launch_vis_scatter(va, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
+  FHS_CUDA(cudaMemcpyAsync(y, st, 2 * op->Mtot * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+// HS_adjoint_operator_G.m:42-57 then real() (precond:
+// HS_adjoint_operator_precond_G.m, x = At(G' (sqrt(pU) .* y))).
+static void adjoint_impl(MeasOp* op, const double* y, double* x, bool precond) {
+  FHS_CHECK(x && y, FHS_ERR_INVALID_ARG, "null buffer");
+  FHS_CHECK(!precond || op->precond, FHS_ERR_STATE, "no preconditioner set");
+  DeviceGuard g(op->device);
+  cudaStream_t s = op->stream;
+  const int64_t N = op->Npix();
+  double* st = stage(op, std::max<int64_t>(N * op->L, 2 * op->Mtot));
+  float* img = img_scratch(op);
+  float2* va = vis_scratch(op, op->vis_a);
+  FHS_CUDA(cudaMemcpyAsync(st, y, 2 * op->Mtot * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_vis_gather(st, va, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
+  if (precond) launch_scale_pu(op, va, true, s);
+  launch_grid_plain(op, 0, op->L, va, s);
+  fft_inverse(op, 0, op->L, s);
+  launch_crop_real(op, img, nullptr, 0, op->L, s);
+  launch_f2d(img, st, N * op->L, s);
+  FHS_CUDA(cudaMemcpyAsync(x, st, N * op->L * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+// util_operator_norm.m:43-61: power iteration on Phi_l^H Phi_l per channel,
+// Phi_l = G_l A (precond: sqrt(pU) G_l A, so the middle factor is pU).
+static void operator_norm_impl(MeasOp* op, int max_iter, double tol, double* sq, bool precond) {
+  FHS_CHECK(sq != nullptr && max_iter > 0, FHS_ERR_INVALID_ARG, "bad arguments");
+  FHS_CHECK(!precond || op->precond, FHS_ERR_STATE, "no preconditioner set");
+  DeviceGuard g(op->device);
+  cudaStream_t s = op->stream;
+  const int64_t N = op->Npix();
+  const int L = op->L;
+  float* img = img_scratch(op);
+  float2* va = vis_scratch(op, op->vis_a);
+  std::vector<float> h((size_t)N * L);
+  std::mt19937_64 rng(12345);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  for (auto& v : h) v = nd(rng);
+  FHS_CUDA(cudaMemcpyAsync(img, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+  DevBuf<double> nrm;
+  nrm.alloc(L);
+  std::vector<double> hn(L), inv(L), val(L, 0.0);
+  std::vector<char> done(L, 0);
+  DevBuf<double> dinv;
+  dinv.alloc(L);
+  launch_plane_sumsq(img, N, L, nrm.p, s);
+  nrm.download(hn.data(), L, s);
+  FHS_CUDA(cudaStreamSynchronize(s));
+  for (int l = 0; l < L; ++l) inv[l] = 1.0 / std::sqrt(hn[l]);
+  dinv.upload(inv.data(), L, s);
+  launch_plane_scale(img, N, L, dinv.p, s);
+  for (int it = 0; it < max_iter; ++it) {
+    launch_pad(op, img, 0, L, s);
+    fft_forward(op, 0, L, s);
+    launch_degrid_plain(op, 0, L, va, s);
+    if (precond) launch_scale_pu(op, va, false, s);
+    launch_grid_plain(op, 0, L, va, s);
+    fft_inverse(op, 0, L, s);
+    launch_crop_real(op, img, nullptr, 0, L, s);
+    launch_plane_sumsq(img, N, L, nrm.p, s);
+    nrm.download(hn.data(), L, s);
+    FHS_CUDA(cudaStreamSynchronize(s));
+    bool all = true;
+    for (int l = 0; l < L; ++l) {
+      const double nv = std::sqrt(hn[l]);
+      FHS_CHECK(std::isfinite(nv), FHS_ERR_NUMERIC, "non-finite operator norm iterate");
+      if (!done[l]) {
+        if (std::fabs(nv - val[l]) <= tol * nv) done[l] = 1;
+        val[l] = nv;
+      }
+      all = all && done[l];
+      inv[l] = nv > 0 ? 1.0 / nv : 0.0;
+    }
+    if (all) break;
+    dinv.upload(inv.data(), L, s);
+    launch_plane_scale(img, N, L, dinv.p, s);
+  }
+  for (int l = 0; l < L; ++l) sq[l] = val[l];
+}
+
 }  // namespace fhs
 
 using namespace fhs;
@@ -177,45 +278,28 @@ fhs_status fhs_apply_adjoint_operator(fhs_measop* op_, int channel, const double
 }
 
 fhs_status fhs_forward_operator(fhs_measop* op_, const double* x, double* y) {
-  return guarded([&] {
-    MeasOp* op = committed(op_);
-    FHS_CHECK(x && y, FHS_ERR_INVALID_ARG, "null buffer");
-    DeviceGuard g(op->device);
-    cudaStream_t s = op->stream;
-    const int64_t N = op->Npix();
-    double* st = stage(op, std::max<int64_t>(N * op->L, 2 * op->Mtot));
-    float* img = img_scratch(op);
-    float2* va = vis_scratch(op, op->vis_a);
-    FHS_CUDA(cudaMemcpyAsync(st, x, N * op->L * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_d2f(st, img, N * op->L, s);
-    launch_pad(op, img, 0, op->L, s);
-    fft_forward(op, 0, op->L, s);
-    launch_degrid_plain(op, 0, op->L, va, s);
-    launch_vis_scatter(va, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
-    FHS_CUDA(cudaMemcpyAsync(y, st, 2 * op->Mtot * sizeof(double), cudaMemcpyDeviceToHost, s));
-    FHS_CUDA(cudaStreamSynchronize(s));
-  });
+  return guarded([&] { forward_impl(committed(op_), x, y, false); });
 }
 
 fhs_status fhs_adjoint_operator(fhs_measop* op_, const double* y, double* x) {
-  return guarded([&] {
-    MeasOp* op = committed(op_);
-    FHS_CHECK(x && y, FHS_ERR_INVALID_ARG, "null buffer");
-    DeviceGuard g(op->device);
-    cudaStream_t s = op->stream;
-    const int64_t N = op->Npix();
-    double* st = stage(op, std::max<int64_t>(N * op->L, 2 * op->Mtot));
-    float* img = img_scratch(op);
-    float2* va = vis_scratch(op, op->vis_a);
-    FHS_CUDA(cudaMemcpyAsync(st, y, 2 * op->Mtot * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_vis_gather(st, va, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
-    launch_grid_plain(op, 0, op->L, va, s);
-    fft_inverse(op, 0, op->L, s);
-    launch_crop_real(op, img, nullptr, 0, op->L, s);
-    launch_f2d(img, st, N * op->L, s);
-    FHS_CUDA(cudaMemcpyAsync(x, st, N * op->L * sizeof(double), cudaMemcpyDeviceToHost, s));
-    FHS_CUDA(cudaStreamSynchronize(s));
-  });
+  return guarded([&] { adjoint_impl(committed(op_), y, x, false); });
+}
+
+fhs_status fhs_forward_operator_precond(fhs_measop* op_, const double* x, double* y) {
+  return guarded([&] { forward_impl(committed(op_), x, y, true); });
+}
+
+fhs_status fhs_adjoint_operator_precond(fhs_measop* op_, const double* y, double* x) {
+  return guarded([&] { adjoint_impl(committed(op_), y, x, true); });
+}
+
+fhs_status fhs_measop_set_preconditioner(fhs_measop* op_, int channel, const double* pU) {
+  return guarded([&] { measop_set_preconditioner(committed(op_), channel, pU); });
+}
+
+fhs_status fhs_gen_preconditioning_matrix(int64_t n_vis, const double* om_y, const double* om_x, int Ky, int Kx,
+                                          int sub_pixels, double* pU) {
+  return guarded([&] { gen_uniform_weights(n_vis, om_y, om_x, Ky, Kx, sub_pixels, pU); });
 }
 
 fhs_status fhs_compute_residual_images(fhs_measop* op_, const double* y, const double* x, double* res) {
@@ -264,59 +348,11 @@ fhs_status fhs_compute_residual_images(fhs_measop* op_, const double* y, const d
 }
 
 fhs_status fhs_operator_norm(fhs_measop* op_, int max_iter, double tol, double* sq) {
-  return guarded([&] {
-    MeasOp* op = committed(op_);
-    FHS_CHECK(sq != nullptr && max_iter > 0, FHS_ERR_INVALID_ARG, "bad arguments");
-    DeviceGuard g(op->device);
-    cudaStream_t s = op->stream;
-    const int64_t N = op->Npix();
-    const int L = op->L;
-    float* img = img_scratch(op);
-    float2* va = vis_scratch(op, op->vis_a);
-    std::vector<float> h((size_t)N * L);
-    std::mt19937_64 rng(12345);
-    std::normal_distribution<float> nd(0.f, 1.f);
-    for (auto& v : h) v = nd(rng);
-    FHS_CUDA(cudaMemcpyAsync(img, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s));
-    DevBuf<double> nrm;
-    nrm.alloc(L);
-    std::vector<double> hn(L), inv(L), val(L, 0.0);
-    std::vector<char> done(L, 0);
-    DevBuf<double> dinv;
-    dinv.alloc(L);
-    launch_plane_sumsq(img, N, L, nrm.p, s);
-    nrm.download(hn.data(), L, s);
-    FHS_CUDA(cudaStreamSynchronize(s));
-    for (int l = 0; l < L; ++l) inv[l] = 1.0 / std::sqrt(hn[l]);
-    dinv.upload(inv.data(), L, s);
-    launch_plane_scale(img, N, L, dinv.p, s);
-    for (int it = 0; it < max_iter; ++it) {
-      launch_pad(op, img, 0, L, s);
-      fft_forward(op, 0, L, s);
-      launch_degrid_plain(op, 0, L, va, s);
-      launch_grid_plain(op, 0, L, va, s);
-      fft_inverse(op, 0, L, s);
-      launch_crop_real(op, img, nullptr, 0, L, s);
-      launch_plane_sumsq(img, N, L, nrm.p, s);
-      nrm.download(hn.data(), L, s);
-      FHS_CUDA(cudaStreamSynchronize(s));
-      bool all = true;
-      for (int l = 0; l < L; ++l) {
-        const double nv = std::sqrt(hn[l]);
-        FHS_CHECK(std::isfinite(nv), FHS_ERR_NUMERIC, "non-finite operator norm iterate");
-        if (!done[l]) {
-          if (std::fabs(nv - val[l]) <= tol * nv) done[l] = 1;
-          val[l] = nv;
-        }
-        all = all && done[l];
-        inv[l] = nv > 0 ? 1.0 / nv : 0.0;
-      }
-      if (all) break;
-      dinv.upload(inv.data(), L, s);
-      launch_plane_scale(img, N, L, dinv.p, s);
-    }
-    for (int l = 0; l < L; ++l) sq[l] = val[l];
-  });
+  return guarded([&] { operator_norm_impl(committed(op_), max_iter, tol, sq, false); });
+}
+
+fhs_status fhs_operator_norm_precond(fhs_measop* op_, int max_iter, double tol, double* sq) {
+  return guarded([&] { operator_norm_impl(committed(op_), max_iter, tol, sq, true); });
 }
 
 }  // extern "C"

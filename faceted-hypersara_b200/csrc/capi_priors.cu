@@ -238,78 +238,144 @@ fhs_status fhs_compute_sara_prior(int device, int Ny, int Nx, int L, int nlevel,
 
 // update_dual_data_fidelity on host buffers: the solver's fused passes with
 // G Fx_old taken from the caller's Fx_old grid (linearity of G).
+}  // extern "C"
+
+namespace fhs {
+namespace {
+
+// src/update_dual_data_fidelity.m:116-147 (no DR) on host buffers: the
+// l2-ball form (pU = 1, :83) or, with precond, the ellipsoid projection
+// (:126-147) warm-started from proj.
+void dual_impl(MeasOp* op, double* v2, double* proj, const double* y, const double* x, double* Fx_old,
+               const double* epsilon, const double* sigma22, double* Ftx, double* norm_res,
+               double* global_norm_res, double* norm_epsilon, bool precond, int max_itr, int min_itr,
+               double stop, int* fb_iters) {
+  FHS_CHECK(v2 && y && x && Fx_old && epsilon && sigma22 && Ftx && norm_res, FHS_ERR_INVALID_ARG,
+            "null argument");
+  FHS_CHECK(op->committed, FHS_ERR_STATE, "operator not committed");
+  if (precond) {
+    FHS_CHECK(proj != nullptr, FHS_ERR_INVALID_ARG, "null proj");
+    FHS_CHECK(op->precond, FHS_ERR_STATE, "no preconditioner set (fhs_measop_set_preconditioner)");
+    FHS_CHECK(max_itr >= 1 && min_itr >= 0 && stop >= 0, FHS_ERR_INVALID_ARG, "bad ellipsoid-projection parameters");
+  }
+  DeviceGuard dg(op->device);
+  cudaStream_t s = op->stream;
+  const int L = op->L;
+  const int64_t N = op->Npix(), No = op->No(), M = op->Mtot;
+  const int64_t stage_n = std::max<int64_t>(std::max<int64_t>(2 * No * L, 2 * M), N * L);
+  if (op->stage.n < (size_t)stage_n) op->stage.alloc(stage_n);
+  if (op->vis_a.n < (size_t)std::max<int64_t>(M, 1)) op->vis_a.alloc(std::max<int64_t>(M, 1));
+  if (op->vis_b.n < (size_t)std::max<int64_t>(M, 1)) op->vis_b.alloc(std::max<int64_t>(M, 1));
+  DevBuf<float2> yd;
+  yd.alloc(std::max<int64_t>(M, 1));
+  DevBuf<double2> wd;
+  if (precond) wd.alloc(std::max<int64_t>(M, 1));
+  DevBuf<float> img, s22;
+  img.alloc(N * L);
+  s22.alloc(L);
+  std::vector<float> hs(sigma22, sigma22 + L);
+  s22.upload(hs.data(), L, s);
+  double* st = op->stage.p;
+  // G Fx_old -> vis_b (gold)
+  FHS_CUDA(cudaMemcpyAsync(st, Fx_old, 2 * No * L * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_grid_from_matlab(st, op->gridA.p, op->Ny, op->Nx, op->Ky, op->Kx, L, s);
+  launch_degrid_plain(op, 0, L, op->vis_b.p, s);
+  // y, v2 -> sorted
+  FHS_CUDA(cudaMemcpyAsync(st, y, 2 * M * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_vis_gather(st, yd.p, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
+  FHS_CUDA(cudaMemcpyAsync(st, v2, 2 * M * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_vis_gather(st, op->vis_a.p, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
+  if (precond) {  // w = proj - y (FP64)
+    FHS_CUDA(cudaMemcpyAsync(st, proj, 2 * M * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_w_from_proj(op, st, yd.p, wd.p, s);
+  }
+  std::vector<double> e((size_t)L * kMaxBlocksPerChannel, 0.0);
+  double eps2 = 0;
+  for (int l = 0; l < L; ++l)
+    for (int b = 0; b < op->h_nblk[l]; ++b) {
+      const double v = epsilon[op->h_blkoff[l] + b];
+      e[(size_t)l * kMaxBlocksPerChannel + b] = v;
+      eps2 += v * v;
+    }
+  op->blk_eps.upload(e.data(), e.size(), s);
+  // A x
+  FHS_CUDA(cudaMemcpyAsync(st, x, N * L * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_d2f(st, img.p, N * L, s);
+  launch_pad(op, img.p, 0, L, s);
+  fft_forward(op, 0, L, s);
+  launch_grid_to_matlab(op->gridA.p, st, op->Ny, op->Nx, op->Ky, op->Kx, L, s);
+  FHS_CUDA(cudaMemcpyAsync(Fx_old, st, 2 * No * L * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+  // fused passes
+  if (precond) {
+    launch_degrid_dual_precond(op, 0, L, op->vis_a.p, op->vis_b.p, yd.p, wd.p, s);
+    launch_block_reduce_precond(op, 0, L, s);
+    launch_fb_iterations(op, 0, L, wd.p, yd.p, max_itr, min_itr, stop, s);
+    launch_grid_dual_precond(op, 0, L, op->vis_a.p, wd.p, s);
+  } else {
+    launch_degrid_dual(op, 0, L, op->vis_a.p, op->vis_b.p, yd.p, s);
+    launch_block_reduce(op, 0, L, s);
+    launch_grid_dual(op, 0, L, op->vis_a.p, s);
+  }
+  fft_inverse(op, 0, L, s);
+  launch_crop_real(op, img.p, s22.p, 0, L, s);
+  launch_f2d(img.p, st, N * L, s);
+  FHS_CUDA(cudaMemcpyAsync(Ftx, st, N * L * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+  launch_vis_scatter(op->vis_a.p, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
+  FHS_CUDA(cudaMemcpyAsync(v2, st, 2 * M * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+  if (precond) {
+    launch_proj_from_w(op, wd.p, yd.p, st, s);
+    FHS_CUDA(cudaMemcpyAsync(proj, st, 2 * M * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  std::vector<double> stats((size_t)op->nblk_tot * 2);
+  op->blk_stats.download(stats.data(), stats.size(), s);
+  std::vector<int> cnt;
+  if (precond && fb_iters) {
+    cnt.resize((size_t)L * kMaxBlocksPerChannel);
+    op->fb_count.download(cnt.data(), cnt.size(), s);
+  }
+  FHS_CUDA(cudaStreamSynchronize(s));
+  double gres = 0;
+  for (int b = 0; b < op->nblk_tot; ++b) {
+    norm_res[b] = std::sqrt(stats[2 * b + 1]);
+    gres += stats[2 * b + 1];
+  }
+  if (precond && fb_iters)
+    for (int l = 0; l < L; ++l)
+      for (int b = 0; b < op->h_nblk[l]; ++b) fb_iters[op->h_blkoff[l] + b] = cnt[(size_t)l * kMaxBlocksPerChannel + b];
+  if (global_norm_res) *global_norm_res = gres;
+  if (norm_epsilon) *norm_epsilon = eps2;
+}
+
+}  // namespace
+}  // namespace fhs
+
+extern "C" {
+
 fhs_status fhs_update_dual_data_fidelity(fhs_measop* op_, double* v2, const double* y, const double* x,
                                          double* Fx_old, const double* epsilon, const double* sigma22,
                                          double* Ftx, double* norm_res, double* global_norm_res,
                                          double* norm_epsilon) {
   return guarded_p([&] {
-    FHS_CHECK(op_ && v2 && y && x && Fx_old && epsilon && sigma22 && Ftx && norm_res, FHS_ERR_INVALID_ARG,
-              "null argument");
-    MeasOp* op = reinterpret_cast<MeasOp*>(op_);
-    FHS_CHECK(op->committed, FHS_ERR_STATE, "operator not committed");
-    DeviceGuard dg(op->device);
-    cudaStream_t s = op->stream;
-    const int L = op->L;
-    const int64_t N = op->Npix(), No = op->No(), M = op->Mtot;
-    const int64_t stage_n = std::max<int64_t>(std::max<int64_t>(2 * No * L, 2 * M), N * L);
-    if (op->stage.n < (size_t)stage_n) op->stage.alloc(stage_n);
-    if (op->vis_a.n < (size_t)std::max<int64_t>(M, 1)) op->vis_a.alloc(std::max<int64_t>(M, 1));
-    if (op->vis_b.n < (size_t)std::max<int64_t>(M, 1)) op->vis_b.alloc(std::max<int64_t>(M, 1));
-    DevBuf<float2> yd;
-    yd.alloc(std::max<int64_t>(M, 1));
-    DevBuf<float> img, s22;
-    img.alloc(N * L);
-    s22.alloc(L);
-    std::vector<float> hs(sigma22, sigma22 + L);
-    s22.upload(hs.data(), L, s);
-    double* st = op->stage.p;
-    // G Fx_old -> vis_b (gold)
-    FHS_CUDA(cudaMemcpyAsync(st, Fx_old, 2 * No * L * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_grid_from_matlab(st, op->gridA.p, op->Ny, op->Nx, op->Ky, op->Kx, L, s);
-    launch_degrid_plain(op, 0, L, op->vis_b.p, s);
-    // y, v2 -> sorted
-    FHS_CUDA(cudaMemcpyAsync(st, y, 2 * M * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_vis_gather(st, yd.p, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
-    FHS_CUDA(cudaMemcpyAsync(st, v2, 2 * M * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_vis_gather(st, op->vis_a.p, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
-    std::vector<double> e((size_t)L * kMaxBlocksPerChannel, 0.0);
-    double eps2 = 0;
-    for (int l = 0; l < L; ++l)
-      for (int b = 0; b < op->h_nblk[l]; ++b) {
-        const double v = epsilon[op->h_blkoff[l] + b];
-        e[(size_t)l * kMaxBlocksPerChannel + b] = v;
-        eps2 += v * v;
-      }
-    op->blk_eps.upload(e.data(), e.size(), s);
-    // A x
-    FHS_CUDA(cudaMemcpyAsync(st, x, N * L * sizeof(double), cudaMemcpyHostToDevice, s));
-    launch_d2f(st, img.p, N * L, s);
-    launch_pad(op, img.p, 0, L, s);
-    fft_forward(op, 0, L, s);
-    launch_grid_to_matlab(op->gridA.p, st, op->Ny, op->Nx, op->Ky, op->Kx, L, s);
-    FHS_CUDA(cudaMemcpyAsync(Fx_old, st, 2 * No * L * sizeof(double), cudaMemcpyDeviceToHost, s));
-    FHS_CUDA(cudaStreamSynchronize(s));
-    // fused passes
-    launch_degrid_dual(op, 0, L, op->vis_a.p, op->vis_b.p, yd.p, s);
-    launch_block_reduce(op, 0, L, s);
-    launch_grid_dual(op, 0, L, op->vis_a.p, s);
-    fft_inverse(op, 0, L, s);
-    launch_crop_real(op, img.p, s22.p, 0, L, s);
-    launch_f2d(img.p, st, N * L, s);
-    FHS_CUDA(cudaMemcpyAsync(Ftx, st, N * L * sizeof(double), cudaMemcpyDeviceToHost, s));
-    FHS_CUDA(cudaStreamSynchronize(s));
-    launch_vis_scatter(op->vis_a.p, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, L, op->maxM, 0, s);
-    FHS_CUDA(cudaMemcpyAsync(v2, st, 2 * M * sizeof(double), cudaMemcpyDeviceToHost, s));
-    std::vector<double> stats((size_t)op->nblk_tot * 2);
-    op->blk_stats.download(stats.data(), stats.size(), s);
-    FHS_CUDA(cudaStreamSynchronize(s));
-    double gres = 0;
-    for (int b = 0; b < op->nblk_tot; ++b) {
-      norm_res[b] = std::sqrt(stats[2 * b + 1]);
-      gres += stats[2 * b + 1];
-    }
-    if (global_norm_res) *global_norm_res = gres;
-    if (norm_epsilon) *norm_epsilon = eps2;
+    FHS_CHECK(op_ != nullptr, FHS_ERR_INVALID_ARG, "null operator handle");
+    dual_impl(reinterpret_cast<MeasOp*>(op_), v2, nullptr, y, x, Fx_old, epsilon, sigma22, Ftx, norm_res,
+              global_norm_res, norm_epsilon, false, 0, 0, 0.0, nullptr);
+  });
+}
+
+fhs_status fhs_update_dual_data_fidelity_precond(fhs_measop* op_, double* v2, double* proj, const double* y,
+                                                 const double* x, double* Fx_old, const double* epsilon,
+                                                 int elipse_proj_max_iter, int elipse_proj_min_iter,
+                                                 double elipse_proj_eps, const double* sigma22, double* Ftx,
+                                                 double* norm_res, double* global_norm_res,
+                                                 double* norm_epsilon, int* fb_iters) {
+  return guarded_p([&] {
+    FHS_CHECK(op_ != nullptr, FHS_ERR_INVALID_ARG, "null operator handle");
+    dual_impl(reinterpret_cast<MeasOp*>(op_), v2, proj, y, x, Fx_old, epsilon, sigma22, Ftx, norm_res,
+              global_norm_res, norm_epsilon, true, elipse_proj_max_iter, elipse_proj_min_iter, elipse_proj_eps,
+              fb_iters);
   });
 }
 

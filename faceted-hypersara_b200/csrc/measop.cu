@@ -74,14 +74,19 @@ __device__ __forceinline__ int wrap(int k, int K) {
 }
 
 // ---------------------------------------------------------------- degrid
-template <int J, bool DUAL>
+// MODE 0: out = G Fx.  MODE 1: l2-ball dual, pass 1.  MODE 2: ellipsoid dual,
+// pass 1 (d = v2/pU + 2 GFx - gold - y to zbuf, block norms of the first FB
+// point t_1 - y = w0 + (mu/pU)(d - w0), w0 = proj - y).
+template <int J, int MODE>
 __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid,
                                                      const WorkItem* __restrict__ items,
                                                      const int* __restrict__ order, int item0,
                                                      float2* __restrict__ out, const float2* __restrict__ v2,
                                                      float2* __restrict__ gold,
                                                      const float2* __restrict__ y,
-                                                     double* __restrict__ partials, float2* __restrict__ zbuf) {
+                                                     double* __restrict__ partials, float2* __restrict__ zbuf,
+                                                     PrecondView pc) {
+  constexpr bool DUAL = MODE != 0;
   // pitch 72 along y: starts within a sub-bin spread over distinct bank pairs
   constexpr int P = kSmemPitch;
   constexpr int R = kTileCells + J - 1;
@@ -132,12 +137,25 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
       const float2 yv = y[vo + i];
       const float2 vv = v2[vo + i];
       const float2 go = gold[vo + i];
-      const float2 z = make_float2(vv.x + 2.f * gfx.x - go.x - yv.x, vv.y + 2.f * gfx.y - go.y - yv.y);
       const float2 r = make_float2(gfx.x - yv.x, gfx.y - yv.y);
-      zbuf[vo + i] = z;
-      gold[vo + i] = gfx;
       const int blk = (int)(kp >> 28);
-      atomicAdd(&bacc[2 * blk], (double)z.x * z.x + (double)z.y * z.y);
+      double n0;
+      if (MODE == 1) {
+        const float2 z = make_float2(vv.x + 2.f * gfx.x - go.x - yv.x, vv.y + 2.f * gfx.y - go.y - yv.y);
+        zbuf[vo + i] = z;
+        n0 = (double)z.x * z.x + (double)z.y * z.y;
+      } else {
+        const float ip = 1.f / pc.pu[vo + i];
+        const float2 d = make_float2(fmaf(vv.x, ip, 2.f * gfx.x - go.x - yv.x),
+                                     fmaf(vv.y, ip, 2.f * gfx.y - go.y - yv.y));
+        zbuf[vo + i] = d;
+        const double2 w0 = pc.w[vo + i];
+        const double m = (double)pc.mu[(size_t)ch * kMaxBlocksPerChannel + blk] * (double)ip;
+        const double tx = fma(m, (double)d.x - w0.x, w0.x), ty = fma(m, (double)d.y - w0.y, w0.y);
+        n0 = tx * tx + ty * ty;
+      }
+      gold[vo + i] = gfx;
+      atomicAdd(&bacc[2 * blk], n0);
       atomicAdd(&bacc[2 * blk + 1], (double)r.x * r.x + (double)r.y * r.y);
     }
   }
@@ -170,7 +188,9 @@ struct BandRange {
   int ring0;  // start rows above the tile (wrap-adjusted offsets)
 };
 
-template <int J, bool DUAL>
+// MODE 0: gridB = G^H vin.  MODE 1: l2-ball dual, pass 2 (v2 = z scale).
+// MODE 2: ellipsoid dual, pass 2 (v2 = pU (d - w), w = proj - y).
+template <int J, int MODE>
 __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __restrict__ gridB,
                                                            const WorkItem* __restrict__ items,
                                                            const int* __restrict__ order, int item0,
@@ -178,7 +198,8 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
                                                            const float2* __restrict__ vin,
                                                            float2* __restrict__ v2,
                                                            const float* __restrict__ blk_scale,
-                                                           const float2* __restrict__ zbuf) {
+                                                           const float2* __restrict__ zbuf, PrecondView pc) {
+  constexpr bool DUAL = MODE != 0;
   static_assert(J <= kMaxTaps && J * J <= 64, "two tap rounds per visibility");
   extern __shared__ float2 gsm2[];
   float2* acc = gsm2;                                           // [kBands][kBandCols][kAccPitch]
@@ -288,11 +309,17 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
         if (r.ring0 && d0 >= 0) d0 -= op.Ky;
         if (warp == 0 && d1 >= 0) d1 -= op.Kx;
         float2 v;
-        if (DUAL) {
+        if (MODE == 1) {
           const float2 z = zbuf[vo + i];
           const float sc = scl[kp >> 28];
           v = make_float2(z.x * sc, z.y * sc);
           if (part == 0 && warp > 0) v2[vo + i] = v;  // the owner tile writes the dual
+        } else if (MODE == 2) {
+          const float2 d = zbuf[vo + i];
+          const double2 w = pc.w[vo + i];
+          const double p = (double)pc.pu[vo + i];
+          v = make_float2((float)(p * ((double)d.x - w.x)), (float)(p * ((double)d.y - w.y)));
+          if (part == 0 && warp > 0) v2[vo + i] = v;
         } else {
           v = vin[vo + i];
         }
@@ -372,22 +399,22 @@ __global__ void __launch_bounds__(256) grid_combine_kernel(OpView op, float2* __
 constexpr size_t kGridSmem = kBands * kBandCols * kAccPitch * sizeof(float2) +
                              kBands * 32 * 2 * kMaxTaps * sizeof(float2) + kBands * 32 * sizeof(int2);
 
-template <int J, bool DUAL>
+template <int J, int MODE>
 void launch_grid_kernel(const MeasOp* op, int c0, int nc, const float2* vin, float2* v2, const float* scale,
-                        const float2* zbuf, cudaStream_t s) {
+                        const float2* zbuf, PrecondView pc, cudaStream_t s) {
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr[dev]) {
-    FHS_CUDA(cudaFuncSetAttribute(grid_kernel<J, DUAL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    FHS_CUDA(cudaFuncSetAttribute(grid_kernel<J, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kGridSmem));
     attr[dev] = true;
   }
   const int i0 = op->h_gr_off[c0], n = op->h_gr_off[c0 + nc] - i0;
   if (n > 0) {
-    grid_kernel<J, DUAL><<<n, kBands * 32, kGridSmem, s>>>(op->view(), op->gridB.p, op->gr_items.p,
+    grid_kernel<J, MODE><<<n, kBands * 32, kGridSmem, s>>>(op->view(), op->gridB.p, op->gr_items.p,
                                                            nullptr, i0, op->gr_partial.p,
-                                                           vin, v2, scale, zbuf);
+                                                           vin, v2, scale, zbuf, pc);
     count_launch();
     FHS_LAUNCH_CHECK();
   }
@@ -435,7 +462,8 @@ __global__ void crop_real_kernel(const float2* __restrict__ grid, float* __restr
 __global__ void block_reduce_kernel(const double* __restrict__ partials, const int* __restrict__ slot_off, int c0,
                                     const int32_t* __restrict__ ch_nblk, const int32_t* __restrict__ ch_blkoff,
                                     const double* __restrict__ blk_eps, float* __restrict__ blk_scale,
-                                    double* __restrict__ blk_stats) {
+                                    double* __restrict__ blk_stats, int mode, double* __restrict__ fb_c,
+                                    int* __restrict__ fb_iter) {
   const int ch = c0 + blockIdx.x;
   const int b = blockIdx.y;
   if (b >= ch_nblk[ch]) return;
@@ -458,10 +486,17 @@ __global__ void block_reduce_kernel(const double* __restrict__ partials, const i
   }
   if (threadIdx.x == 0) {
     const double zn = sqrt(s0[0]);
-    const double eps = blk_eps[(size_t)ch * kMaxBlocksPerChannel + b];
-    // v2 = z (1 - min(eps/||z||, 1))  (update_dual_data_fidelity.m:83)
-    const double sc = zn > 0 ? 1.0 - fmin(eps / zn, 1.0) : 0.0;
-    blk_scale[(size_t)ch * kMaxBlocksPerChannel + b] = (float)sc;
+    const size_t k = (size_t)ch * kMaxBlocksPerChannel + b;
+    const double eps = blk_eps[k];
+    if (mode == 0) {
+      // v2 = z (1 - min(eps/||z||, 1))  (update_dual_data_fidelity.m:83)
+      const double sc = zn > 0 ? 1.0 - fmin(eps / zn, 1.0) : 0.0;
+      blk_scale[k] = (float)sc;
+    } else {
+      // first FB point of the ellipsoid projection: scale of P_B(t_1)
+      fb_c[k] = zn > eps ? eps / zn : 1.0;
+      fb_iter[k] = 0;
+    }
     const int gb = ch_blkoff[ch] + b;
     blk_stats[2 * gb] = s0[0];
     blk_stats[2 * gb + 1] = s1[0];
@@ -799,17 +834,25 @@ void fft_inverse(const MeasOp* op, int p0, int np, cudaStream_t s) {
   fft_exec(op, op->gridB.p, op->gridA.p, p0, np, CUFFT_INVERSE);
 }
 
+PrecondView MeasOp::precond_view(const double2* w) const {
+  PrecondView v;
+  v.pu = pu.p;
+  v.w = w;
+  v.mu = blk_mu.p;
+  return v;
+}
+
 void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s) {
   const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
   if (n == 0) return;
-  degrid_kernel<7, false><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr,
-                                            i0, out, nullptr, nullptr, nullptr, nullptr, nullptr);
+  degrid_kernel<7, 0><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, out, nullptr,
+                                        nullptr, nullptr, nullptr, nullptr, PrecondView{});
   count_launch();
   FHS_LAUNCH_CHECK();
 }
 
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s) {
-  launch_grid_kernel<7, false>(op, c0, nc, v, nullptr, nullptr, nullptr, s);
+  launch_grid_kernel<7, 0>(op, c0, nc, v, nullptr, nullptr, nullptr, PrecondView{}, s);
 }
 
 void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s) {
@@ -824,22 +867,45 @@ void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* go
                         cudaStream_t s) {
   const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
   if (n == 0) return;
-  degrid_kernel<7, true><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr,
-                                           i0, nullptr, v2, gold, y, op->partials.p, op->zbuf.p);
+  degrid_kernel<7, 1><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, nullptr, v2, gold,
+                                        y, op->partials.p, op->zbuf.p, PrecondView{});
   count_launch();
   FHS_LAUNCH_CHECK();
 }
 
-void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s) {
-  dim3 grid(nc, kMaxBlocksPerChannel);
-  block_reduce_kernel<<<grid, 256, 0, s>>>(op->partials.p, op->dg_off.p, c0, op->ch_nblk.p, op->ch_blkoff.p,
-                                           op->blk_eps.p, op->blk_scale.p, op->blk_stats.p);
+void launch_degrid_dual_precond(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold,
+                                const float2* y, const double2* w, cudaStream_t s) {
+  FHS_CHECK(op->precond, FHS_ERR_STATE, "no preconditioner set");
+  const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
+  if (n == 0) return;
+  degrid_kernel<7, 2><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, nullptr, v2, gold,
+                                        y, op->partials.p, op->zbuf.p, op->precond_view(w));
   count_launch();
   FHS_LAUNCH_CHECK();
+}
+
+static void block_reduce(const MeasOp* op, int c0, int nc, int mode, cudaStream_t s) {
+  dim3 grid(nc, kMaxBlocksPerChannel);
+  block_reduce_kernel<<<grid, 256, 0, s>>>(op->partials.p, op->dg_off.p, c0, op->ch_nblk.p, op->ch_blkoff.p,
+                                           op->blk_eps.p, op->blk_scale.p, op->blk_stats.p, mode,
+                                           op->fb_c.p, op->fb_iter.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
+void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s) { block_reduce(op, c0, nc, 0, s); }
+
+void launch_block_reduce_precond(const MeasOp* op, int c0, int nc, cudaStream_t s) {
+  block_reduce(op, c0, nc, 1, s);
 }
 
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s) {
-  launch_grid_kernel<7, true>(op, c0, nc, nullptr, v2, op->blk_scale.p, op->zbuf.p, s);
+  launch_grid_kernel<7, 1>(op, c0, nc, nullptr, v2, op->blk_scale.p, op->zbuf.p, PrecondView{}, s);
+}
+
+void launch_grid_dual_precond(const MeasOp* op, int c0, int nc, float2* v2, const double2* w, cudaStream_t s) {
+  FHS_CHECK(op->precond, FHS_ERR_STATE, "no preconditioner set");
+  launch_grid_kernel<7, 2>(op, c0, nc, nullptr, v2, nullptr, op->zbuf.p, op->precond_view(w), s);
 }
 
 }  // namespace fhs

@@ -35,6 +35,18 @@ struct WorkItem {
   int pad;
 };
 
+// Preconditioned (ellipsoid) dual: pointers read by the tile kernels.
+struct PrecondView {
+  const float* pu = nullptr;    // [Mtot] diagonal preconditioner pU (sorted order)
+  const double2* w = nullptr;   // [Mtot] proj - y, the ellipsoid-projection iterate
+  const float* mu = nullptr;    // [L][kMaxBlocksPerChannel] FB step: min of pU over the block
+};
+
+// A chunk of one channel's visibilities for the ellipsoid FB passes.
+struct FbItem {
+  int ch, beg, end, pad;
+};
+
 struct GridCombine {
   int ch, tile, pbase, nsplit;
 };
@@ -96,10 +108,27 @@ struct MeasOp {
   DevBuf<float> blk_scale;  // [L][kMaxBlocksPerChannel]
   DevBuf<double> blk_eps;   // [L][kMaxBlocksPerChannel]
 
+  // preconditioning (set_preconditioner) and the ellipsoid projection state
+  bool precond = false;
+  std::vector<char> pu_set;               // [L]
+  std::vector<float> h_mu;                // [L][kMaxBlocksPerChannel]
+  int max_nblk = 1;                       // most blocks in any channel
+  DevBuf<float> pu;                       // [Mtot] sorted order
+  DevBuf<uint8_t> vblk;                   // [Mtot] block of each sorted visibility
+  DevBuf<float> blk_mu;                   // [L][kMaxBlocksPerChannel]
+  DevBuf<double> fb_c;                    // [L][kMaxBlocksPerChannel] scale of the next projection
+  DevBuf<int> fb_iter;                    // [L][kMaxBlocksPerChannel] FB iterations done, -1 finished
+  DevBuf<int> fb_count;                   // [L][kMaxBlocksPerChannel] FB iterations of the last call
+  DevBuf<FbItem> fb_items;
+  std::vector<int> h_fb_off;              // [L+1] FB items per channel
+  DevBuf<int> fb_off;
+  DevBuf<double> fb_part;                 // [fb items][kMaxBlocksPerChannel][3]
+
   int64_t No() const { return (int64_t)Ky * Kx; }
   int64_t Npix() const { return (int64_t)Ny * Nx; }
   int ntiles() const { return nT0 * nT1; }
   OpView view() const;
+  PrecondView precond_view(const double2* w) const;
   ~MeasOp();
 };
 
@@ -127,5 +156,28 @@ void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* go
 void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s);
 // fused dual update, pass 2: v2 <- zbuf*scale, gridB <- G^H v2
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s);
+
+// ---- preconditioned dual (ellipsoid projection, see ellipse.cu) ---------
+// pU of one channel in its original visibility order (requires a committed op)
+void measop_set_preconditioner(MeasOp* op, int channel, const double* pu);
+// pass 1: d = v2/pU + 2 GFx - gold - y -> zbuf, GFx -> gold, ||t_1 - y||^2 partials
+void launch_degrid_dual_precond(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold,
+                                const float2* y, const double2* w, cudaStream_t s);
+// block norms -> scale of the first projection, FB counters reset
+void launch_block_reduce_precond(const MeasOp* op, int c0, int nc, cudaStream_t s);
+// max_itr forward-backward passes (finished blocks skip their visibilities)
+void launch_fb_iterations(const MeasOp* op, int c0, int nc, double2* w, const float2* y, int max_itr,
+                          int min_itr, double stop, cudaStream_t s);
+// pass 2: v2 = pU (d - w), gridB <- G^H v2
+void launch_grid_dual_precond(const MeasOp* op, int c0, int nc, float2* v2, const double2* w, cudaStream_t s);
+// w = z - y for a given z (z NULL: z = 0); z = w + y back in original visibility order (double)
+void launch_w_from_proj(const MeasOp* op, const double* z_host_layout, const float2* y, double2* w,
+                        cudaStream_t s);
+void launch_proj_from_w(const MeasOp* op, const double2* w, const float2* y, double* z_host_layout,
+                        cudaStream_t s);
+// v <- sqrt(pU) .* v (root) or pU .* v (sorted order, all channels)
+void launch_scale_pu(const MeasOp* op, float2* v, bool root, cudaStream_t s);
+// util_gen_preconditioning_matrix, uniform weighting (host)
+void gen_uniform_weights(int64_t n, const double* om_y, const double* om_x, int Ky, int Kx, int sub, double* pu);
 
 }  // namespace fhs

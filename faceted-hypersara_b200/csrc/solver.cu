@@ -223,7 +223,8 @@ Solver::~Solver() {
   if (graph) cudaGraphExecDestroy(graph);
 }
 
-static const char* kStageNames[] = {"primal_pad", "fft_forward", "degrid_dual", "block_reduce", "grid_dual",
+static const char* kStageNames[] = {"primal_pad", "fft_forward", "degrid_dual", "block_reduce", "ellipse_fb",
+                                    "grid_dual",
                                     "fft_inverse", "sara_analysis_prox", "l21_prox", "sara_synthesis", "facet_gram",
                                     "facet_eig", "facet_reconstruct", "assemble_g", "stats"};
 constexpr int kStages = sizeof(kStageNames) / sizeof(kStageNames[0]);
@@ -245,12 +246,24 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   mark();
   fft_forward(op, 0, L, s);
   mark();
-  launch_degrid_dual(op, 0, L, S->v2.p, S->gold.p, S->y.p, s);
-  mark();
-  launch_block_reduce(op, 0, L, s);
-  mark();
-  launch_grid_dual(op, 0, L, S->v2.p, s);
-  mark();
+  if (S->precond) {
+    launch_degrid_dual_precond(op, 0, L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s);
+    mark();
+    launch_block_reduce_precond(op, 0, L, s);
+    mark();
+    launch_fb_iterations(op, 0, L, S->projw.p, S->y.p, S->fb_max, S->fb_min, S->fb_stop, s);
+    mark();
+    launch_grid_dual_precond(op, 0, L, S->v2.p, S->projw.p, s);
+    mark();
+  } else {
+    launch_degrid_dual(op, 0, L, S->v2.p, S->gold.p, S->y.p, s);
+    mark();
+    launch_block_reduce(op, 0, L, s);
+    mark();
+    mark();
+    launch_grid_dual(op, 0, L, S->v2.p, s);
+    mark();
+  }
   fft_inverse(op, 0, L, s);
   mark();
   FHS_CUDA(cudaMemsetAsync(S->l21_acc.p, 0, S->G * sizeof(double), s));
@@ -517,6 +530,17 @@ fhs_status fhs_solver_set_params(fhs_solver* s_, const fhs_solver_params* p) {
     S->pdfb_rel_var = p->pdfb_rel_var;
     S->pdfb_tol = p->pdfb_fidelity_tolerance;
     S->pdfb_rel_var_low = p->pdfb_rel_var_low;
+    if (p->elipse_proj_max_iter > 0) {
+      FHS_CHECK(p->elipse_proj_min_iter >= 0 && p->elipse_proj_eps >= 0, FHS_ERR_INVALID_ARG,
+                "bad ellipsoid-projection parameters");
+      S->fb_max = p->elipse_proj_max_iter;
+      S->fb_min = p->elipse_proj_min_iter;
+      S->fb_stop = p->elipse_proj_eps;
+    } else {  // imaging/default_parameters.json "proj"
+      S->fb_max = 20;
+      S->fb_min = 1;
+      S->fb_stop = 1e-8;
+    }
     const double sigma0 = 1.0 / p->nu0, sigma1 = 1.0 / p->nu1;
     // facetHyperSARA.m:582-608 / hyperSARA.m:471-487: tau = 0.99/3;
     // sara.m:502-505: tau = 0.99/(sigma1 nu1 + sigma2 nu2) = 0.99/2
@@ -572,6 +596,18 @@ fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
     launch_pad(op, S->x.p, 0, S->L, s);
     fft_forward(op, 0, S->L, s);
     launch_degrid_plain(op, 0, S->L, S->gold.p, s);
+    S->precond = op->precond;
+    if (S->precond) {
+      if (S->projw.n < (size_t)std::max<int64_t>(op->Mtot, 1)) S->projw.alloc(std::max<int64_t>(op->Mtot, 1));
+      launch_w_from_proj(op, nullptr, S->y.p, S->projw.p, s);  // proj = 0 (fhs_initialize_data_worker.m:43)
+      if (S->algo == FHS_ALGO_SARA) {
+        // sara.m:420-428: proj starts as the projection of G A x0 from zero.
+        // With v2 = 0 and gold = G A x0 the dual pass 1 gives d = G A x0 - y.
+        launch_degrid_dual_precond(op, 0, S->L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s);
+        launch_block_reduce_precond(op, 0, S->L, s);
+        launch_fb_iterations(op, 0, S->L, S->projw.p, S->y.p, S->fb_max, S->fb_min, S->fb_stop, s);
+      }
+    }
     solver_update_weights(S);
     FHS_CUDA(cudaStreamSynchronize(s));
     solver_capture(S);

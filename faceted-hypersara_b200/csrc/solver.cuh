@@ -21,6 +21,10 @@ struct Solver {
   DevBuf<float> x, g, xhat, g1, coef, apx, v1, w1, v0, rownorm;
   DevBuf<double> beta1, w0, beta0, sig_bar, sig;
   DevBuf<float2> y, v2, gold;
+  DevBuf<double2> projw;        // proj - y of the ellipsoid projection (preconditioned operator)
+  bool precond = false;         // operator carried a preconditioner at init
+  int fb_max = 20, fb_min = 1;  // elipse_proj_max_iter / min_iter
+  double fb_stop = 1e-8;        // elipse_proj_eps
   DevBuf<float> sigma22;
   DevBuf<double> primal_part;   // [L][kPrimalBlocks][2]
   DevBuf<double> l21_part;      // [G][prox blocks] (unfused prox path)

@@ -42,7 +42,9 @@ class SolverParams(C.Structure):
                 ("reweighting_min_iter", C.c_int), ("reweighting_max_iter", C.c_int),
                 ("reweighting_rel_var", C.c_double), ("pdfb_min_iter", C.c_int),
                 ("pdfb_max_iter", C.c_int), ("pdfb_rel_var", C.c_double),
-                ("pdfb_fidelity_tolerance", C.c_double), ("pdfb_rel_var_low", C.c_double)]
+                ("pdfb_fidelity_tolerance", C.c_double), ("pdfb_rel_var_low", C.c_double),
+                ("elipse_proj_max_iter", C.c_int), ("elipse_proj_min_iter", C.c_int),
+                ("elipse_proj_eps", C.c_double)]
 
 
 class IterInfo(C.Structure):
@@ -80,6 +82,14 @@ SIGNATURES = {
     "fhs_operator_norm": (C.c_int, [_vp, C.c_int, C.c_double, _dp]),
     "fhs_compute_residual_images": (C.c_int, [_vp, _dp, _dp, _dp]),
     "fhs_update_dual_data_fidelity": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+    "fhs_gen_preconditioning_matrix": (C.c_int, [C.c_int64, _dp, _dp, C.c_int, C.c_int, C.c_int, _dp]),
+    "fhs_measop_set_preconditioner": (C.c_int, [_vp, C.c_int, _dp]),
+    "fhs_forward_operator_precond": (C.c_int, [_vp, _dp, _dp]),
+    "fhs_adjoint_operator_precond": (C.c_int, [_vp, _dp, _dp]),
+    "fhs_operator_norm_precond": (C.c_int, [_vp, C.c_int, C.c_double, _dp]),
+    "fhs_update_dual_data_fidelity_precond": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_int,
+                                                        C.c_double, _dp, _dp, _dp, _dp, _dp,
+                                                        C.POINTER(C.c_int)]),
     "fhs_proj_l2ball": (C.c_int, [C.c_int, C.c_int64, _dp, C.c_double, _dp, _dp]),
     "fhs_proj_l2ball_noalloc": (C.c_int, [C.c_int, C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                           C.c_void_p]),

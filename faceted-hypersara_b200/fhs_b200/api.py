@@ -5,7 +5,10 @@ Function names, argument meaning and return values follow the reference
 
 * ``apply_direct_operator`` / ``apply_adjoint_operator``  (src/apply_*_operator.m:1)
 * ``HS_forward_operator_G`` / ``HS_adjoint_operator_G``   (lib/operators/HS_*_operator_G.m:1)
-* ``update_dual_data_fidelity``                           (src/update_dual_data_fidelity.m:1-6)
+* ``update_dual_data_fidelity`` (pU = 1) and ``update_dual_data_fidelity_precond``
+                                                          (src/update_dual_data_fidelity.m:1-6)
+* ``HS_forward_operator_precond_G`` / ``HS_adjoint_operator_precond_G``,
+  ``gen_preconditioning_matrix``                          (lib/operators/, util_gen_preconditioning_matrix)
 * ``proj_l2ball``, ``nuclear_norm``, ``compute_sara_prior`` (src/*.m:1)
 * ``facetHyperSARA``, ``hyperSARA``, ``sara``              (src/{fhs,hs,sara}/*.m:1)
 
@@ -120,10 +123,25 @@ class MeasurementOperator:
         return np.concatenate([np.asarray(b, dtype=np.complex128).ravel() for b in yl]) if len(yl) else \
             np.zeros(0, np.complex128)
 
-    def operator_norm(self, max_iter=200, tol=1e-8):
+    def operator_norm(self, max_iter=200, tol=1e-8, precond=False):
+        """Per-channel squared norms of G_l A (precond: of sqrt(pU) G_l A),
+        lib/utils/util_operator_norm.m:43-61."""
         out = np.empty(self.L)
-        check(lib().fhs_operator_norm(self._h, max_iter, tol, dptr(out)))
+        fn = lib().fhs_operator_norm_precond if precond else lib().fhs_operator_norm
+        check(fn(self._h, max_iter, tol, dptr(out)))
         return out
+
+    def set_preconditioner(self, pU):
+        """Attach aW: ``pU[l]`` is one channel's preconditioner, either one
+        array over its visibilities or a list over its blocks."""
+        if len(pU) != self.L:
+            raise ValueError(f"expected {self.L} channels of preconditioner")
+        for l, pl in enumerate(pU):
+            a = _f64(np.concatenate([np.asarray(b, dtype=np.float64).ravel() for b in pl])
+                     if isinstance(pl, (list, tuple)) else np.asarray(pl, dtype=np.float64).ravel())
+            if a.size != self.n_vis[l]:
+                raise ValueError(f"channel {l}: expected {self.n_vis[l]} preconditioner entries, got {a.size}")
+            check(lib().fhs_measop_set_preconditioner(self._h, l, dptr(a)))
 
 
 # ------------------------------------------------------------------ functions
@@ -162,6 +180,39 @@ def HS_adjoint_operator_G(y, op: MeasurementOperator):
     x = np.empty(op.Ny * op.Nx * op.L)
     check(lib().fhs_adjoint_operator(op.handle, dptr(flat), dptr(x)))
     return x.reshape(op.Ny, op.Nx, op.L, order="F")
+
+
+def HS_forward_operator_precond_G(x, op: MeasurementOperator):
+    """lib/operators/HS_forward_operator_precond_G.m:40-55: sqrt(aW) .* G A x -> y[l][b]."""
+    x = _cube_in(x, op.Ny, op.Nx)
+    y = np.empty(op.n_vis_total, dtype=np.complex128)
+    check(lib().fhs_forward_operator_precond(op.handle, dptr(x.reshape(-1, order="F")),
+                                             dptr(y.view(np.float64))))
+    out, pos = [], 0
+    for l in range(op.L):
+        out.append(op.split(l, y[pos:pos + op.n_vis[l]]))
+        pos += op.n_vis[l]
+    return out
+
+
+def HS_adjoint_operator_precond_G(y, op: MeasurementOperator):
+    """lib/operators/HS_adjoint_operator_precond_G.m: real(At(G' (sqrt(aW) .* y))) -> [Ny, Nx, L]."""
+    flat = _cplx_in(np.concatenate([op.flatten(yl) for yl in y]))
+    x = np.empty(op.Ny * op.Nx * op.L)
+    check(lib().fhs_adjoint_operator_precond(op.handle, dptr(flat), dptr(x)))
+    return x.reshape(op.Ny, op.Nx, op.L, order="F")
+
+
+def gen_preconditioning_matrix(om_y, om_x, Ky, Kx, sub_pixels=1):
+    """util_gen_preconditioning_matrix with gen_uniform_weight_matrix = true:
+    pU = 1 / (visibilities in the same cell of a (Ky sub) x (Kx sub) grid)."""
+    omy, omx = _f64(om_y).ravel(), _f64(om_x).ravel()
+    if omy.size != omx.size:
+        raise ValueError("om_y and om_x differ in length")
+    out = np.empty(omy.size)
+    check(lib().fhs_gen_preconditioning_matrix(omy.size, dptr(omy), dptr(omx), int(Ky), int(Kx),
+                                               int(sub_pixels), dptr(out)))
+    return out
 
 
 def compute_residual_images(x, y, op: MeasurementOperator):
@@ -271,11 +322,51 @@ def update_dual_data_fidelity(v2, y, x, Fx_old, op: MeasurementOperator, epsilon
             float(neps[0]))
 
 
+def update_dual_data_fidelity_precond(v2, y, x, Fx_old, proj, op: MeasurementOperator, epsilon,
+                                      elipse_proj_max_iter, elipse_proj_min_iter, elipse_proj_eps, sigma22):
+    """src/update_dual_data_fidelity.m:1-6, 126-147 (no DR) with the
+    operator's preconditioner (``op.set_preconditioner``).
+
+    Returns (v2, Ftx, Fx_old, proj, norm_res, global_norm_res, norm_epsilon,
+    fb_iters), the reference's outputs plus the FB iterations per block."""
+    xc = _cube_in(x, op.Ny, op.Nx)
+    v2f = _cplx_in(np.concatenate([op.flatten(v) for v in v2])).copy()
+    pjf = _cplx_in(np.concatenate([op.flatten(v) for v in proj])).copy()
+    yf = _cplx_in(np.concatenate([op.flatten(v) for v in y]))
+    Fo = np.asfortranarray(np.asarray(Fx_old, dtype=np.complex128).reshape(op.No, op.L, order="F"))
+    Fo_flat = np.ascontiguousarray(Fo.T).view(np.float64).copy()
+    eps = np.concatenate([np.asarray(e, dtype=np.float64).ravel() for e in epsilon])
+    s22 = _f64(np.broadcast_to(np.asarray(sigma22, dtype=np.float64), (op.L,)))
+    Ftx = np.empty(op.Ny * op.Nx * op.L)
+    nres = np.empty(eps.size)
+    gres = np.zeros(1)
+    neps = np.zeros(1)
+    its = np.zeros(eps.size, dtype=np.int32)
+    check(lib().fhs_update_dual_data_fidelity_precond(
+        op.handle, dptr(v2f), dptr(pjf), dptr(yf), dptr(xc.reshape(-1, order="F")), dptr(Fo_flat), dptr(eps),
+        int(elipse_proj_max_iter), int(elipse_proj_min_iter), float(elipse_proj_eps), dptr(s22), dptr(Ftx),
+        dptr(nres), dptr(gres), dptr(neps), its.ctypes.data_as(C.POINTER(C.c_int))))
+    v2c, pjc = v2f.view(np.complex128), pjf.view(np.complex128)
+    v2_out, pj_out, nr_out, it_out, pos, bpos = [], [], [], [], 0, 0
+    for l in range(op.L):
+        v2_out.append(op.split(l, v2c[pos:pos + op.n_vis[l]]))
+        pj_out.append(op.split(l, pjc[pos:pos + op.n_vis[l]]))
+        nb = len(op.block_sizes[l])
+        nr_out.append(list(nres[bpos:bpos + nb]))
+        it_out.append([int(v) for v in its[bpos:bpos + nb]])
+        pos += op.n_vis[l]
+        bpos += nb
+    Fx_new = Fo_flat.view(np.complex128).reshape(op.L, op.No).T.copy(order="F")
+    return (v2_out, Ftx.reshape(op.Ny, op.Nx, op.L, order="F"), Fx_new, pj_out, nr_out, float(gres[0]),
+            float(neps[0]), it_out)
+
+
 # ------------------------------------------------------------------- solvers
 _PARAM_DEFAULTS = dict(
     nu0=1.0, nu1=1.0, reweighting_alpha=1.0, reweighting_flag=True, reweighting_min_iter=1,
     reweighting_max_iter=20, reweighting_rel_var=1e-4, pdfb_min_iter=10, pdfb_max_iter=2000,
-    pdfb_rel_var=5e-5, pdfb_fidelity_tolerance=1.01, pdfb_rel_var_low=5e-6)
+    pdfb_rel_var=5e-5, pdfb_fidelity_tolerance=1.01, pdfb_rel_var_low=5e-6,
+    elipse_proj_max_iter=20, elipse_proj_min_iter=1, elipse_proj_eps=1e-8)
 
 
 class Solver:
@@ -283,7 +374,9 @@ class Solver:
 
     ``param``: dict with the reference's ``param`` fields (imaging/imaging.m:839-860):
     nu2 [L], gamma (per group), gamma0 (per group x facet), reweighting_sig,
-    reweighting_sig_bar, reweighting_*, pdfb_*.
+    reweighting_sig_bar, reweighting_*, pdfb_*, elipse_proj_*.  A solver
+    initialised on an operator with a preconditioner runs the ellipsoid
+    projection (the reference's default data term), else the l2-ball form.
     """
 
     def __init__(self, op: MeasurementOperator, algo: int, param: dict, nlevel=4, n_groups=1, Qy=1, Qx=1,
@@ -339,6 +432,9 @@ class Solver:
         sp.pdfb_rel_var = float(p["pdfb_rel_var"])
         sp.pdfb_fidelity_tolerance = float(p["pdfb_fidelity_tolerance"])
         sp.pdfb_rel_var_low = float(p["pdfb_rel_var_low"])
+        sp.elipse_proj_max_iter = int(p["elipse_proj_max_iter"])
+        sp.elipse_proj_min_iter = int(p["elipse_proj_min_iter"])
+        sp.elipse_proj_eps = float(p["elipse_proj_eps"])
         check(lib().fhs_solver_set_params(self._h, C.byref(sp)))
 
     def set_data(self, y, epsilon):
@@ -404,7 +500,8 @@ def facetHyperSARA(y, epsilon, op: MeasurementOperator, param: dict, Qx, Qy, nle
                    window_type="triangular", overlap_size=(0, 0), xinit=None, n_groups=1, splits_y=None,
                    splits_x=None, max_iter=0):
     """src/fhs/facetHyperSARA.m:1-6 -> (xsol [Ny, Nx, L], info).  The
-    reference's A, At, G, W are the operator handle; pU = 1; no DR."""
+    reference's A, At, G, W are the operator handle and pU its preconditioner
+    (none: pU = 1); no DR."""
     s = Solver(op, LB.ALGO_FHS, param, nlevel, n_groups, Qy, Qx, overlap_size, window_type, splits_y, splits_x)
     try:
         s.set_data(y, epsilon)

@@ -110,6 +110,45 @@ FHS_API fhs_status fhs_update_dual_data_fidelity(fhs_measop* op, double* v2, con
                                          const double* sigma22, double* Ftx, double* norm_res,
                                          double* global_norm_res, double* norm_epsilon);
 
+/* ----------------------------------------------------------------------
+ * Preconditioning and the ellipsoid projection (default non-DR data term of
+ * the reference: src/update_dual_data_fidelity.m:126-147,
+ * src/sara/sara.m:561-562,594-595)
+ * ---------------------------------------------------------------------- */
+/* util_gen_preconditioning_matrix (RI-measurement-operator submodule, set up
+ * at imaging/imaging.m:436-438) with gen_uniform_weight_matrix = true:
+ * pU[m] = 1 / (number of visibilities in the cell of visibility m on a
+ * (Ky sub_pixels) x (Kx sub_pixels) grid, cells centred on the grid points).
+ * Host computation over n_vis frequencies (radians). */
+FHS_API fhs_status fhs_gen_preconditioning_matrix(int64_t n_vis, const double* om_y, const double* om_x, int Ky,
+                                                  int Kx, int sub_pixels, double* pU);
+/* Attaches the diagonal preconditioner aW{l} of one channel (all blocks, in
+ * the channel's visibility order; entries finite and > 0).  Needs a committed
+ * operator.  Once every channel has one, the *_precond calls below work and a
+ * solver initialised afterwards runs the ellipsoid projection. */
+FHS_API fhs_status fhs_measop_set_preconditioner(fhs_measop* op, int channel, const double* pU);
+/* lib/operators/HS_forward_operator_precond_G.m:40-55: y = sqrt(pU) .* G A x. */
+FHS_API fhs_status fhs_forward_operator_precond(fhs_measop* op, const double* x, double* y);
+/* lib/operators/HS_adjoint_operator_precond_G.m: x = real(At(G' (sqrt(pU) .* y))). */
+FHS_API fhs_status fhs_adjoint_operator_precond(fhs_measop* op, const double* y, double* x);
+/* lib/utils/util_operator_norm.m:46-52: per-channel ||sqrt(pU) G_l A||^2
+ * (squared_operator_norm_precond, the nu2 of imaging/imaging.m:846). */
+FHS_API fhs_status fhs_operator_norm_precond(fhs_measop* op, int max_iter, double tol, double* squared_norms);
+/* src/update_dual_data_fidelity.m:126-147 (no DR) on host buffers:
+ * proj = solver_proj_elipse_fb(v2 ./ pU, r2, y, pU, eps, proj, max, min, eps_stop),
+ * v2 = v2 + pU .* (r2 - proj), forward-backward iterations with step
+ * mu = min(pU) per block, stopped when ||proj_k - proj_{k-1}|| <= eps_stop
+ * ||proj_k|| after at least min iterations or at max iterations.  Arguments
+ * as fhs_update_dual_data_fidelity plus proj (in/out, all visibilities) and
+ * fb_iters (optional out, FB iterations run per block). */
+FHS_API fhs_status fhs_update_dual_data_fidelity_precond(fhs_measop* op, double* v2, double* proj,
+                                                         const double* y, const double* x, double* Fx_old,
+                                                         const double* epsilon, int elipse_proj_max_iter,
+                                                         int elipse_proj_min_iter, double elipse_proj_eps,
+                                                         const double* sigma22, double* Ftx, double* norm_res,
+                                                         double* global_norm_res, double* norm_epsilon,
+                                                         int* fb_iters);
+
 /* ======================================================================
  * Priors (standalone, device selected per call)
  * ====================================================================== */
@@ -184,6 +223,10 @@ typedef struct fhs_solver_params {
   double reweighting_rel_var;
   int pdfb_min_iter, pdfb_max_iter;
   double pdfb_rel_var, pdfb_fidelity_tolerance, pdfb_rel_var_low;
+  /* ellipsoid projection (used when the operator carries a preconditioner);
+   * elipse_proj_max_iter <= 0 selects 20 / 1 / 1e-8 for all three */
+  int elipse_proj_max_iter, elipse_proj_min_iter;
+  double elipse_proj_eps;
 } fhs_solver_params;
 
 /* Per-iteration record (FP64), summed over all groups. */

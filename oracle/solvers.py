@@ -3,10 +3,17 @@
 TEST INFRASTRUCTURE ONLY (see ``oracle/nufft.py``).
 
 Arrays are channel-first here: an image cube is ``x[L, Ny, Nx]``.  Each
-function cites the reference file it restates.  The preconditioning matrices
-``pU`` are identity (the l2-ball form ``update_dual_data_fidelity.m:83``
-reached by ``solver_proj_elipse_fb`` when ``pU = 1``), and visibility gridding
-(DR) is off.
+function cites the reference file it restates.  The data-fidelity dual takes
+either the l2-ball form (``pU = 1``, ``update_dual_data_fidelity.m:83``) or,
+with a ``Precond``, the preconditioned ellipsoid projection
+(``update_dual_data_fidelity.m:126-147``).  Visibility gridding (DR) is off.
+
+The ellipsoid projection ``solver_proj_elipse_fb`` and the uniform-weight
+preconditioner ``util_gen_preconditioning_matrix`` belong to the
+RI-measurement-operator submodule, which the reference tree does not vendor;
+both are restated from the published method (Onose et al. 2017) and pinned by
+their optimality conditions and the ``pU = 1`` reduction only (parity of
+those two functions against the reference is unpinned).
 """
 from __future__ import annotations
 
@@ -63,23 +70,28 @@ class DataTerm:
         return len(self.G)
 
 
-def forward_operator(x, data: DataTerm):
-    """lib/operators/HS_forward_operator_G.m:36-52 (no DR)."""
+def forward_operator(x, data: DataTerm, pU=None):
+    """lib/operators/HS_forward_operator_G.m:36-52 (no DR); with pU,
+    HS_forward_operator_precond_G.m:40-55: sqrt(pU) .* (G A x)."""
     out = []
     for l in range(data.L):
         Fx = data.op.A(x[l])
-        out.append([G @ Fx for G in data.G[l]])
+        if pU is None:
+            out.append([G @ Fx for G in data.G[l]])
+        else:
+            out.append([np.sqrt(pu) * (G @ Fx) for G, pu in zip(data.G[l], pU[l])])
     return out
 
 
-def adjoint_operator(yb, data: DataTerm):
-    """lib/operators/HS_adjoint_operator_G.m:42-57 (no DR), real part kept."""
+def adjoint_operator(yb, data: DataTerm, pU=None):
+    """lib/operators/HS_adjoint_operator_G.m:42-57 (no DR), real part kept;
+    with pU, HS_adjoint_operator_precond_G.m: At(G' (sqrt(pU) .* y))."""
     op = data.op
     out = np.zeros((data.L, op.Ny, op.Nx))
     for l in range(data.L):
         g2 = np.zeros(op.No, dtype=np.complex128)
-        for G, v in zip(data.G[l], yb[l]):
-            g2 += G.conj().T @ v
+        for b, (G, v) in enumerate(zip(data.G[l], yb[l])):
+            g2 += G.conj().T @ (v if pU is None else np.sqrt(pU[l][b]) * v)
         out[l] = np.real(op.At(g2))
     return out
 
@@ -207,9 +219,10 @@ def compute_residual_images(x, data: DataTerm):
     return out
 
 
-def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0):
+def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0, pU=None):
     """Squared spectral norm of Phi_l = G_l A per channel by power iteration
-    (lib/utils/util_operator_norm.m:43-61, op_norm of the missing submodule)."""
+    (lib/utils/util_operator_norm.m:43-61, op_norm of the missing submodule);
+    with pU, of sqrt(pU) G_l A (util_operator_norm.m:46-52)."""
     rng = np.random.default_rng(seed)
     op = data.op
     out = np.zeros(data.L)
@@ -220,8 +233,8 @@ def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0):
         for _ in range(n_iter):
             Fx = op.A(x)
             g2 = np.zeros(op.No, dtype=np.complex128)
-            for G in data.G[l]:
-                g2 += G.conj().T @ (G @ Fx)
+            for b, G in enumerate(data.G[l]):
+                g2 += G.conj().T @ (G @ Fx if pU is None else pU[l][b] * (G @ Fx))
             xn = np.real(op.At(g2))
             new = np.linalg.norm(xn)
             x = xn / new
@@ -334,9 +347,29 @@ def _stop_pdfb(t, last, rel, res, epsn, p: SolverParams):
         or rel <= p.pdfb_rel_var_low)
 
 
+@dataclass
+class Precond:
+    """Preconditioning matrices pU[l][b] (diagonal, one vector per block) and
+    the ``elipse_proj_*`` parameters (imaging/default_parameters.json)."""
+    pU: list
+    max_itr: int = 20
+    min_itr: int = 1
+    stop: float = 1e-8
+
+
+def _dual_step(v2, proj, x, Fx_old, data, sigma22, pc: Precond | None):
+    if pc is None:
+        v2, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, sigma22)
+        return v2, proj, Ftx, Fx_old, gres, geps
+    v2, proj, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity_precond(
+        v2, proj, x, Fx_old, data, pc.pU, sigma22, pc.max_itr, pc.min_itr, pc.stop)
+    return v2, proj, Ftx, Fx_old, gres, geps
+
+
 def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
-                    xinit=None, max_iter=None, callback=None):
-    """src/fhs/facetHyperSARA.m:701-1138 (one spectral sub-cube, pU = 1)."""
+                    xinit=None, max_iter=None, callback=None, precond: Precond | None = None):
+    """src/fhs/facetHyperSARA.m:701-1138 (one spectral sub-cube); proj starts
+    at zero (src/fhs/fhs_initialize_data_worker.m:43)."""
     op = data.op
     L = data.L
     x = np.zeros((L, op.Ny, op.Nx)) if xinit is None else np.array(xinit, dtype=np.float64)
@@ -359,6 +392,7 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
     v1 = np.zeros((L, s))
     w1 = np.ones(s) if zero else l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
     v2 = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
+    proj = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
     Fx_old = np.stack([op.A(x[l]) for l in range(L)])
     g = np.zeros_like(x)
     log = SolverLog()
@@ -367,7 +401,7 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
     max_iter = max_iter or (p.reweighting_max_iter + 1) * p.pdfb_max_iter
     for t in range(1, max_iter + 1):
         x, xhat, rel_x, norm_x = primal_update(x, g)
-        v2, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, sigma22)
+        v2, proj, Ftx, Fx_old, gres, geps = _dual_step(v2, proj, x, Fx_old, data, sigma22, precond)
         gacc = np.zeros_like(x)
         for q, (y0, y1), (x0, x1), win in facets:
             v0[q], g0 = nuclear_prox_update(v0[q], xhat[:, y0:y1, x0:x1], win, w0[q], beta0[q])
@@ -397,18 +431,22 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
     return x, log
 
 
-def hypersara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None):
-    """src/hs/hyperSARA.m:565-866 (no faceting, pU = 1)."""
+def hypersara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None,
+              precond: Precond | None = None):
+    """src/hs/hyperSARA.m:565-866 (no faceting)."""
     op = data.op
     geom = FacetGeometry(op.Ny, op.Nx, 1, 1, (0, 0), window_type="none")
     # HyperSARA is the Q = 1 faceted iteration without window; its g0 scaling
     # (sigma0 inside hs_update_dual_lowrankness_serial.m:42) equals sigma00
     # because hyperSARA.m:476 also builds sigma00 = tau*sigma0.
-    return facet_hypersara(data, p, geom, xinit, max_iter, callback)
+    return facet_hypersara(data, p, geom, xinit, max_iter, callback, precond)
 
 
-def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None):
-    """src/sara/sara.m:521-837 (single channel, per-basis l1 prox)."""
+def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None,
+         precond: Precond | None = None):
+    """src/sara/sara.m:521-837 (single channel, per-basis l1 prox).  With a
+    preconditioner, proj starts as the projection of G A x0 from zero
+    (src/sara/sara.m:420-428)."""
     op = data.op
     assert data.L == 1
     x = np.zeros((1, op.Ny, op.Nx)) if xinit is None else np.array(xinit, dtype=np.float64).reshape(1, op.Ny, op.Nx)
@@ -422,6 +460,11 @@ def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=No
     v1 = np.zeros_like(w1)
     v2 = [[np.zeros_like(yb) for yb in data.y[0]]]
     Fx_old = np.stack([op.A(x[0])])
+    proj = None
+    if precond is not None:
+        proj = [[proj_ellipse_fb(G @ Fx_old[0], yb, pu, e, np.zeros_like(yb), precond.max_itr,
+                                 precond.min_itr, precond.stop)[0]
+                 for G, yb, pu, e in zip(data.G[0], data.y[0], precond.pU[0], data.eps[0])]]
     g = np.zeros_like(x)
     log = SolverLog()
     x_last_rw = x.copy()
@@ -432,7 +475,7 @@ def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=No
         r1 = v1 + wv.sara_analysis(xhat[0], p.nlevel)                # run_par_waverec
         v1 = r1 - np.sign(r1) * np.maximum(np.abs(r1) - beta1 * w1, 0.0)
         g1 = wv.sara_synthesis(v1, op.Ny, op.Nx, p.nlevel)
-        v2, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, [1.0])
+        v2, proj, Ftx, Fx_old, gres, geps = _dual_step(v2, proj, x, Fx_old, data, [1.0], precond)
         g = sigma11 * g1[None] + sigma22 * Ftx                        # sara.m:633
         rel = np.sqrt(rel_x / norm_x) if norm_x > 0 else 0.0
         res, epsn = np.sqrt(gres), np.sqrt(geps)

@@ -31,8 +31,9 @@ def test_abi_version_and_cpu_only_calls():
     for n0, n1 in ((64, 64), (37, 29), (1024, 1024)):
         assert L.fhs_sara_n_coefs(n0, n1, 4) == wavelets.n_coefs_sara(n0, n1)
     assert L.fhs_sara_n_coefs(8, 8, 0) == -1
-    assert L.fhs_solver_stage_count() == 14
+    assert L.fhs_solver_stage_count() == 15
     assert L.fhs_solver_stage_name(2) == b"degrid_dual"
+    assert L.fhs_solver_stage_name(4) == b"ellipse_fb"
 
 
 def test_errors_are_reported_not_raised():

@@ -215,3 +215,33 @@ def test_small_fhs_solve_improves_snr():
     x, log = so.facet_hypersara(data, p, geom)
     assert so.snr_db(xt, x) > 8.0
     assert log.n_reweights == 1
+
+
+def test_ellipse_projection_optimality_and_l2ball_reduction():
+    """proj_ellipse_fb solves min (z-s)^H diag(1/pU) (z-s) s.t. ||z-y|| <= eps:
+    on the sphere its KKT condition is (s - z)/pU = lam (z - y), lam >= 0; with
+    pU = 1 one iteration is the l2-ball projection; inside the ball z = s."""
+    rng = np.random.default_rng(4)
+    n = 300
+    y = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    s = y + 3.0 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    pU = rng.uniform(0.2, 1.0, n)
+    z, k = so.proj_ellipse_fb(s, y, pU, 10.0, np.zeros(n), max_itr=500, min_itr=1, stop=1e-12)
+    assert abs(np.linalg.norm(z - y) - 10.0) < 1e-9
+    lam = ((s - z) / pU) / (z - y)
+    assert np.std(lam.real) < 1e-6 * abs(np.mean(lam.real)) and np.mean(lam.real) > 0
+    assert np.max(np.abs(lam.imag)) < 1e-6
+    z1, k1 = so.proj_ellipse_fb(s, y, np.ones(n), 10.0, np.zeros(n), 20, 1, 1e-10)
+    assert np.allclose(z1, so.proj_l2ball(s, 10.0, y), atol=1e-12)
+    zin, _ = so.proj_ellipse_fb(y + 0.01 * (s - y), y, pU, 10.0, np.zeros(n), 2000, 1, 1e-13)
+    assert np.allclose(zin, y + 0.01 * (s - y), atol=1e-9)
+
+
+def test_uniform_weight_preconditioner_counts():
+    Ky = Kx = 16
+    # three points in cell (1, 2), one in (0, 0), one on the wrapped edge (15 -> cell 15)
+    g = 2 * np.pi / 16
+    om_y = np.array([1 * g, 1.2 * g, 0.8 * g, 0.0, -1 * g])
+    om_x = np.array([2 * g, 2.3 * g, 1.9 * g, 0.1 * g, 0.0])
+    pU = so.uniform_weight_preconditioner(om_y, om_x, Ky, Kx)
+    assert np.allclose(pU, [1 / 3, 1 / 3, 1 / 3, 1.0, 1.0])
