@@ -145,8 +145,11 @@ def _barrier(dist, local):
         torch.cuda.synchronize(local)
 
 
-def algorithmic_bytes(prob, sp_s):
-    """Algorithmic HBM bytes per launch of each hand-written stage, whole cube."""
+def algorithmic_bytes(prob, sp_s, fb_counts=None):
+    """Algorithmic HBM bytes per launch of each hand-written stage, whole cube.
+    With a preconditioner the dual passes also read pU (f32) and proj - y
+    (f64 complex), and each FB iteration of a block streams 53 B per
+    visibility (w read+write 32, d 8, y 8, pU 4, block id 1)."""
     op = prob["op"]
     L, N, M = op.L, op.Ny * op.Nx, prob["n_vis"]
     No = op.No
@@ -156,10 +159,11 @@ def algorithmic_bytes(prob, sp_s):
     from fhs_b200.heuristics import facet_pixels
     P = sum(facet_pixels(sy, sx, (ov, ov)))
     s_w = sp_s - N
-    return {
+    pre = 20 if prob.get("precond") else 0
+    out = {
         "primal_pad": N * L * (4 + 4) + N * L * (4 + 4 + 8),
-        "degrid_dual": No * L * 8 + M * (16 + 8 + 8 + 8) + M * (8 + 8),
-        "grid_dual": M * (16 + 8) + M * 8 + No * L * 8,
+        "degrid_dual": No * L * 8 + M * (16 + 8 + 8 + 8 + pre) + M * (8 + 8),
+        "grid_dual": M * (16 + 8 + pre) + M * 8 + No * L * 8,
         "sara_analysis": N * L * 4 + s_w * L * 4,
         "l21_prox": 2 * sp_s * L * 4 + s_w * L * 4 + N * L * 4 + sp_s * 4 * prob["C"],
         "sara_synthesis": sp_s * L * 4 + N * L * 4,
@@ -167,6 +171,9 @@ def algorithmic_bytes(prob, sp_s):
         "facet_reconstruct": 3 * P * L * 4,
         "assemble_g": N * L * (8 + 4 + 4) + P * L * 4,
     }
+    if fb_counts is not None:
+        out["ellipse_fb"] = sum(k * m * 53 for kl, bl in zip(fb_counts, op.block_sizes) for k, m in zip(kl, bl))
+    return out
 
 
 def _traffic_from_profiles(kernel):
@@ -258,7 +265,7 @@ def run_ours(args):
     from fhs_b200.workload import build_problem, make_solver
     seed = 1000 + rank
     wl = {"small": SMALL, "medium": MEDIUM}.get(args.case, WORKLOAD)
-    prob = build_problem(**wl, seed=seed, device=local)
+    prob = build_problem(**wl, seed=seed, device=local, precond=args.precond)
     s = make_solver(prob)
     s.init()
     s.iterate(args.warmup, record=False)
@@ -277,7 +284,8 @@ def run_ours(args):
     # ---- per-stage device times (same stream, stage-by-stage launches)
     stages = s.profile_stages(3)
     from fhs_b200 import sara_n_coefs
-    nbytes = algorithmic_bytes(prob, sara_n_coefs(wl["Ny"], wl["Nx"], 4))
+    nbytes = algorithmic_bytes(prob, sara_n_coefs(wl["Ny"], wl["Nx"], 4),
+                               s.ellipse_iterations() if args.precond else None)
     mine = {k: v for k, v in stages.items() if k in nbytes}
     dom = max(mine, key=mine.get)
     peak, peak_kind = _peaks()
@@ -307,13 +315,16 @@ def run_ours(args):
                "sample": "one FHS iteration of the FP64 oracle on 1 channel at 1024x1024 (its full visibility "
                          "set, 4x4 facets), scaled by 64 channels"}
     if rank == 0:
+        if args.precond:  # variant line: the reference's default preconditioned data term
+            stage_rows["ellipse_fb_iterations_mean"] = float(np.mean([k for kl in s.ellipse_iterations() for k in kl]))
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": _config({"visibilities": prob["n_vis"], "parallelism": f"{world} independent cubes"})
                 if args.case == "full" else {"workload": f"fhs_{wl['Ny']}x{wl['Nx']}x{wl['L']}_C4_Q4x4 (profiling case)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-                "clocks": clocks, "stages_ms": stage_rows,
+                "clocks": clocks, "stages_ms": stage_rows, "data_term": "ellipsoid projection, uniform-weight pU"
+                if args.precond else "l2 ball (pU = 1)",
                 "vis_per_s": 2.0 * prob["n_vis"] * value}
         print(json.dumps(line), flush=True)
     s.close()
@@ -355,7 +366,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", choices=["full", "medium", "small"], default="full",
                     help="medium (512x512x64) / small (512x512x16): profiling cases for ncu captures, not bench lines")
+    ap.add_argument("--precond", action="store_true",
+                    help="variant: uniform-weight preconditioner and the ellipsoid projection (not the bench line)")
     args = ap.parse_args()
+    if args.precond:
+        args.no_cpu_baseline = True
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -37,6 +37,7 @@ namespace {
 constexpr int kFbThreads = 256;
 constexpr int kFbWarps = kFbThreads / 32;
 constexpr int kFbChunk = 8192;  // visibilities per CTA and pass
+constexpr int kFbUnroll = 4;    // visibilities in flight per thread
 
 int blocks_for(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>((n + 255) / 256, 1), 148 * 16); }
 
@@ -69,32 +70,63 @@ __global__ void __launch_bounds__(kFbThreads) fb_advance_kernel(
   }
   __syncthreads();
   if (!any) return;  // every block of the channel has stopped (uniform across the CTA)
-  double acc[NB][3];
+  // ||t - y||^2 sets the next scale: FP64 (its rounding must not jitter the
+  // iterate); the stopping-test sums only need FP32 per thread
+  double acc0[NB];
+  float acc1[NB], acc2[NB];
 #pragma unroll
-  for (int k = 0; k < NB; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+  for (int k = 0; k < NB; ++k) {
+    acc0[k] = 0.0;
+    acc1[k] = acc2[k] = 0.f;
+  }
   const int64_t vo = ch_voff[it.ch];
-  for (int i = it.beg + threadIdx.x; i < it.end; i += kFbThreads) {
-    const int b = vblk[vo + i];
-    if (!s_act[b]) continue;
-    const float ip = 1.f / pu[vo + i];
-    const double m = (double)s_mu[b] * (double)ip;
-    const float2 d = dbuf[vo + i];
-    const double2 wp = w[vo + i];
-    const double c = s_c[b];
-    const double2 t = fb_point(wp, d, m);
-    const double2 wn = make_double2(c * t.x, c * t.y);
-    w[vo + i] = wn;
-    const float2 yv = y[vo + i];
-    const double2 tn = fb_point(wn, d, m);
-    const double dx = wn.x - wp.x, dy = wn.y - wp.y;
-    const double zx = wn.x + (double)yv.x, zy = wn.y + (double)yv.y;
-    const double q0 = tn.x * tn.x + tn.y * tn.y, q1 = dx * dx + dy * dy, q2 = zx * zx + zy * zy;
+  // kFbUnroll visibilities per thread and step: their loads are issued
+  // together (the block id first, then the operands of the active ones)
+  for (int base = it.beg + threadIdx.x; base < it.end; base += kFbThreads * kFbUnroll) {
+    int bl[kFbUnroll];
+    bool act[kFbUnroll];
 #pragma unroll
-    for (int k = 0; k < NB; ++k) {
-      if (b == k) {
-        acc[k][0] += q0;
-        acc[k][1] += q1;
-        acc[k][2] += q2;
+    for (int u = 0; u < kFbUnroll; ++u) {
+      const int i = base + u * kFbThreads;
+      bl[u] = i < it.end ? (int)vblk[vo + i] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kFbUnroll; ++u) act[u] = (base + u * kFbThreads < it.end) && s_act[bl[u]];
+    float ip[kFbUnroll];
+    float2 d[kFbUnroll], yv[kFbUnroll];
+    double2 wp[kFbUnroll];
+#pragma unroll
+    for (int u = 0; u < kFbUnroll; ++u) {
+      if (act[u]) {
+        const int64_t i = vo + base + u * kFbThreads;
+        ip[u] = pu[i];
+        d[u] = dbuf[i];
+        wp[u] = w[i];
+        yv[u] = y[i];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kFbUnroll; ++u) {
+      if (!act[u]) continue;
+      const int b = bl[u];
+      const float inv = 1.f / ip[u];
+      const double m = (double)s_mu[b] * (double)inv;
+      const double c = s_c[b];
+      const double2 t = fb_point(wp[u], d[u], m);
+      const double2 wn = make_double2(c * t.x, c * t.y);
+      w[vo + base + u * kFbThreads] = wn;
+      const double2 tn = fb_point(wn, d[u], m);
+      const double dx = wn.x - wp[u].x, dy = wn.y - wp[u].y;
+      const double zx = wn.x + (double)yv[u].x, zy = wn.y + (double)yv[u].y;
+      const double q0 = tn.x * tn.x + tn.y * tn.y;
+      const float q1 = (float)(dx * dx + dy * dy), q2 = (float)(zx * zx + zy * zy);
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        if (b == k) {
+          acc0[k] += q0;
+          acc1[k] += q1;
+          acc2[k] += q2;
+        }
       }
     }
   }
@@ -103,7 +135,7 @@ __global__ void __launch_bounds__(kFbThreads) fb_advance_kernel(
   for (int k = 0; k < NB; ++k) {
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
-      double v = acc[k][f];
+      double v = f == 0 ? acc0[k] : (double)(f == 1 ? acc1[k] : acc2[k]);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (lane == 0) red[warp][k * 3 + f] = v;
@@ -311,12 +343,17 @@ void launch_fb_iterations(const MeasOp* op, int c0, int nc, double2* w, const fl
   const int nb = op->max_nblk;
   for (int k = 0; k < max_itr; ++k) {
     if (n > 0) {
+      // per-thread accumulators for every block of a channel: the fewest that fit
       if (nb <= 1)
         advance<1>(op, i0, n, w, y, s);
       else if (nb <= 2)
         advance<2>(op, i0, n, w, y, s);
+      else if (nb <= 3)
+        advance<3>(op, i0, n, w, y, s);
       else if (nb <= 4)
         advance<4>(op, i0, n, w, y, s);
+      else if (nb <= 6)
+        advance<6>(op, i0, n, w, y, s);
       else if (nb <= 8)
         advance<8>(op, i0, n, w, y, s);
       else

@@ -742,6 +742,22 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
   });
 }
 
+fhs_status fhs_solver_ellipse_iterations(fhs_solver* s_, int* counts) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(counts != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    MeasOp* op = S->op;
+    std::vector<int> c((size_t)op->L * kMaxBlocksPerChannel, 0);
+    if (S->precond) {
+      DeviceGuard dg(op->device);
+      op->fb_count.download(c.data(), c.size(), op->stream);
+      FHS_CUDA(cudaStreamSynchronize(op->stream));
+    }
+    for (int l = 0; l < op->L; ++l)
+      for (int b = 0; b < op->h_nblk[l]; ++b) counts[op->h_blkoff[l] + b] = c[(size_t)l * kMaxBlocksPerChannel + b];
+  });
+}
+
 int fhs_solver_stage_count(void) { return kStages; }
 
 const char* fhs_solver_stage_name(int i) { return (i >= 0 && i < kStages) ? kStageNames[i] : ""; }

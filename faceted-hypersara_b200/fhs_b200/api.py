@@ -466,6 +466,18 @@ class Solver:
     def update_weights(self):
         check(lib().fhs_solver_update_weights(self._h))
 
+    def ellipse_iterations(self):
+        """FB iterations of the ellipsoid projection per block in the last
+        iteration (nested [l][b]; zeros without a preconditioner)."""
+        n = sum(len(b) for b in self.op.block_sizes)
+        out = np.zeros(n, dtype=np.int32)
+        check(lib().fhs_solver_ellipse_iterations(self._h, out.ctypes.data_as(C.POINTER(C.c_int))))
+        res, pos = [], 0
+        for bs in self.op.block_sizes:
+            res.append([int(v) for v in out[pos:pos + len(bs)]])
+            pos += len(bs)
+        return res
+
     def time_iterations(self, n):
         """Device milliseconds of n graph replays (CUDA events on the solver stream)."""
         ms = np.zeros(1)

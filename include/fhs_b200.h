@@ -264,6 +264,11 @@ FHS_API fhs_status fhs_solver_iterate(fhs_solver* s, int n, fhs_iter_info* info)
  * (reweighting_max_iter+1)*pdfb_max_iter). */
 FHS_API fhs_status fhs_solver_run(fhs_solver* s, int max_iter, fhs_run_info* info);
 FHS_API fhs_status fhs_solver_get_x(fhs_solver* s, double* x);
+/* Forward-backward iterations of the ellipsoid projection in the most recent
+ * iteration, one per block (channel-major); all 0 without a preconditioner.
+ * The reference's solver_proj_elipse_fb returns the same count as its second
+ * output (src/sara/sara.m:561). */
+FHS_API fhs_status fhs_solver_ellipse_iterations(fhs_solver* s, int* counts);
 /* Recompute reweighting weights from the current x (fhs_update_weights.m). */
 FHS_API fhs_status fhs_solver_update_weights(fhs_solver* s);
 
