@@ -402,9 +402,22 @@ void launch_analysis_prox(dim3 grid, cudaStream_t s, const LevelArgs& a, const f
 }
 
 // ----------------------------------------------------------- synthesis
-constexpr int ST0 = 32, ST1 = 16;                          // output tile (y, x)
-constexpr int SP0 = ST0 / 2 + kSaraMaxFilter / 2;          // 24 coefficient rows
-constexpr int SP1 = ST1 / 2 + kSaraMaxFilter / 2;          // 16
+// One synthesis level is the adjoint of an analysis level: with an even tile
+// start, the output pair (2k, 2k+1) along an axis draws on the same LF/2
+// coefficients c[k..k+LF/2-1]:
+//   out[2k] = sum_j c[k+j] f[2j+1],   out[2k+1] = sum_j c[k+j] f[2j]
+// (f = Lo_D or Hi_D, t = 2p + 1 - i of the full-convolution adjoint).  A CTA
+// owns a 64 (y) x 32 (x) output tile: it stages the four subbands' coefficient
+// window (32 + LF/2 - 1 rows x 16 + LF/2 - 1 columns), filters along y (one
+// thread per column and output pair) into shared memory, then along x (one
+// thread per output row, 8 output columns in registers).  The filter length
+// is a template parameter selected per basis, so both filters live in
+// registers.  Final level: the CTA loops over the 8 bases, accumulating in
+// registers, and adds the Dirac part; coarser levels write one basis each.
+constexpr int SY = 64, SX = 32;                         // output tile (y, x)
+constexpr int SRY = SY / 2 + kSaraMaxFilter / 2 - 1;    // 39 coefficient rows
+constexpr int SRX = SX / 2 + kSaraMaxFilter / 2 - 1;    // 23 coefficient columns
+constexpr int SRYP = SRY + 1;                           // row pitch of the window
 
 struct SynArgs {
   int m0[kSaraWavelets], m1[kSaraWavelets];    // coefficient sizes (level j)
@@ -420,87 +433,129 @@ struct SynArgs {
   float alpha;
 };
 
-// Accumulates the synthesis of basis b for the output tile into acc[2].
+struct SynSmem {
+  float sub[4][SRX][SRYP];   // A, H, V, D coefficient windows
+  float tl[SRX][SY];         // y-filtered low  (A lo + H hi)
+  float th[SRX][SY];         // y-filtered high (V lo + D hi)
+};
+
+// Adds basis b's synthesis of the tile at (I0s, I1s) to acc[q] (output row
+// threadIdx.x % 64, column 8 (threadIdx.x / 64) + q).
+template <int LF>
 __device__ __forceinline__ void syn_basis(const SynArgs& a, int b, int plane, const float* __restrict__ coef,
-                                          const float* __restrict__ apx, int I0s, int I1s,
-                                          float (*sub)[SP1][SP0], float (*tlo)[ST0], float (*thi)[ST0],
-                                          float acc[2]) {
-  const int Lf = 2 * (b + 1);
+                                          const float* __restrict__ apx, int I0s, int I1s, SynSmem& S,
+                                          float acc[8]) {
+  constexpr int H = LF / 2;
+  constexpr int RY = SY / 2 + H - 1, RX = SX / 2 + H - 1;
+  float lo[LF], hi[LF];
+#pragma unroll
+  for (int t = 0; t < LF; ++t) {
+    lo[t] = c_lo[b][t];
+    hi[t] = c_hi[b][t];
+  }
   const int m0 = a.m0[b], m1 = a.m1[b];
   const int P0s = I0s / 2, P1s = I1s / 2;
-  const int P0n = (I0s + ST0 - 1 + Lf - 2) / 2 - P0s + 1;
-  const int P1n = (I1s + ST1 - 1 + Lf - 2) / 2 - P1s + 1;
   const float* A = (a.a_from_coef ? coef + (size_t)plane * a.s_stride : apx + (size_t)plane * a.apx_stride) +
                    a.a_off[b];
-  const float* H = coef + (size_t)plane * a.s_stride + a.h_off[b];
+  const float* Hc = coef + (size_t)plane * a.s_stride + a.h_off[b];
   const size_t mm = (size_t)m0 * m1;
-  for (int idx = threadIdx.x; idx < P0n * P1n; idx += blockDim.x) {
-    const int l1 = idx / P0n, l0 = idx - l1 * P0n;
+  for (int idx = threadIdx.x; idx < RY * RX; idx += blockDim.x) {
+    const int l1 = idx / RY, l0 = idx - l1 * RY;
     const int p0 = P0s + l0, p1 = P1s + l1;
     float va = 0.f, vh = 0.f, vv = 0.f, vd = 0.f;
     if (p0 < m0 && p1 < m1) {
       const size_t o = (size_t)p1 * m0 + p0;
       va = A[o];
-      vh = H[o];
-      vv = H[mm + o];
-      vd = H[2 * mm + o];
+      vh = Hc[o];
+      vv = Hc[mm + o];
+      vd = Hc[2 * mm + o];
     }
-    sub[0][l1][l0] = va;
-    sub[1][l1][l0] = vh;
-    sub[2][l1][l0] = vv;
-    sub[3][l1][l0] = vd;
+    S.sub[0][l1][l0] = va;
+    S.sub[1][l1][l0] = vh;
+    S.sub[2][l1][l0] = vv;
+    S.sub[3][l1][l0] = vd;
   }
   __syncthreads();
-  // along y: tlo/thi[p1][i0]
-  for (int idx = threadIdx.x; idx < P1n * ST0; idx += blockDim.x) {
-    const int l1 = idx / ST0, li0 = idx - l1 * ST0;
-    const int i0 = I0s + li0;
-    float lo = 0.f, hi = 0.f;
-    const int pa = i0 / 2, pb = (i0 + Lf - 2) / 2;
-    for (int p0 = pa; p0 <= pb; ++p0) {
-      const int t = 2 * p0 + 1 - i0;
-      const int l0 = p0 - P0s;
-      lo = fmaf(sub[0][l1][l0], c_lo[b][t], fmaf(sub[1][l1][l0], c_hi[b][t], lo));
-      hi = fmaf(sub[2][l1][l0], c_lo[b][t], fmaf(sub[3][l1][l0], c_hi[b][t], hi));
+  // along y: task = (column l1, output pair k), k fastest
+  for (int task = threadIdx.x; task < RX * (SY / 2); task += blockDim.x) {
+    const int l1 = task / (SY / 2), k = task - l1 * (SY / 2);
+    float le = 0.f, lo_ = 0.f, he = 0.f, ho = 0.f;
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      const float ca = S.sub[0][l1][k + j], ch = S.sub[1][l1][k + j];
+      const float cv = S.sub[2][l1][k + j], cd = S.sub[3][l1][k + j];
+      le = fmaf(ca, lo[2 * j + 1], fmaf(ch, hi[2 * j + 1], le));
+      lo_ = fmaf(ca, lo[2 * j], fmaf(ch, hi[2 * j], lo_));
+      he = fmaf(cv, lo[2 * j + 1], fmaf(cd, hi[2 * j + 1], he));
+      ho = fmaf(cv, lo[2 * j], fmaf(cd, hi[2 * j], ho));
     }
-    tlo[l1][li0] = lo;
-    thi[l1][li0] = hi;
+    *reinterpret_cast<float2*>(&S.tl[l1][2 * k]) = make_float2(le, lo_);
+    *reinterpret_cast<float2*>(&S.th[l1][2 * k]) = make_float2(he, ho);
   }
   __syncthreads();
-  const int li0 = threadIdx.x % ST0;
-  for (int r = 0; r < 2; ++r) {
-    const int li1 = threadIdx.x / ST0 + 8 * r;
-    const int i1 = I1s + li1;
-    float v = 0.f;
-    const int pa = i1 / 2, pb = (i1 + Lf - 2) / 2;
-    for (int p1 = pa; p1 <= pb; ++p1) {
-      const int t = 2 * p1 + 1 - i1;
-      v = fmaf(tlo[p1 - P1s][li0], c_lo[b][t], fmaf(thi[p1 - P1s][li0], c_hi[b][t], v));
-    }
-    acc[r] += v;
+  // along x: output row i0, pairs m = 4 grp + q (columns 2m, 2m+1)
+  const int i0 = threadIdx.x % SY, grp = threadIdx.x / SY;
+  float cl[H + 3], ch[H + 3];
+#pragma unroll
+  for (int c = 0; c < H + 3; ++c) {
+    cl[c] = S.tl[4 * grp + c][i0];
+    ch[c] = S.th[4 * grp + c][i0];
   }
-  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float e = 0.f, o = 0.f;
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      e = fmaf(cl[q + j], lo[2 * j + 1], fmaf(ch[q + j], hi[2 * j + 1], e));
+      o = fmaf(cl[q + j], lo[2 * j], fmaf(ch[q + j], hi[2 * j], o));
+    }
+    acc[2 * q] += e;
+    acc[2 * q + 1] += o;
+  }
+  // No barrier before the next basis: its window load rewrites sub, whose
+  // last reads (the y pass) precede this basis's second barrier, and its y
+  // pass rewrites tl/th only after its first barrier, which every thread
+  // reaches after finishing this x pass.
 }
 
-__global__ void __launch_bounds__(256) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
+__device__ __forceinline__ void syn_dispatch(const SynArgs& a, int b, int plane, const float* __restrict__ coef,
+                                             const float* __restrict__ apx, int I0s, int I1s, SynSmem& S,
+                                             float acc[8]) {
+  switch (b) {
+    case 0: syn_basis<2>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 1: syn_basis<4>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 2: syn_basis<6>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 3: syn_basis<8>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 4: syn_basis<10>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 5: syn_basis<12>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 6: syn_basis<14>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    default: syn_basis<16>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+  }
+}
+
+__global__ void __launch_bounds__(256, 3) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
                                                         float* __restrict__ apx, float* __restrict__ out) {
-  __shared__ float sub[4][SP1][SP0];
-  __shared__ float tlo[SP1][ST0];
-  __shared__ float thi[SP1][ST0];
+  __shared__ SynSmem S;
   const int plane = blockIdx.z;
   const int tile = blockIdx.x;
+  const int i0 = threadIdx.x % SY, grp = threadIdx.x / SY;
+  float acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc[q] = 0.f;
   if (!a.final_level) {
     const int b = blockIdx.y;
     if (tile >= a.tiles[b]) return;
     const int ti0 = tile % a.tiles0[b], ti1 = tile / a.tiles0[b];
-    const int I0s = ti0 * ST0, I1s = ti1 * ST1;
-    float acc[2] = {0.f, 0.f};
-    syn_basis(a, b, plane, coef, apx, I0s, I1s, sub, tlo, thi, acc);
+    const int I0s = ti0 * SY, I1s = ti1 * SX;
+    syn_dispatch(a, b, plane, coef, apx, I0s, I1s, S, acc);
     const int n0 = a.n0[b], n1 = a.n1[b];
-    const int li0 = threadIdx.x % ST0;
-    for (int r = 0; r < 2; ++r) {
-      const int i0 = I0s + li0, i1 = I1s + threadIdx.x / ST0 + 8 * r;
-      if (i0 < n0 && i1 < n1) apx[(size_t)plane * a.apx_stride + a.out_off[b] + (size_t)i1 * n0 + i0] = acc[r];
+    float* dst = apx + (size_t)plane * a.apx_stride + a.out_off[b];
+    if (I0s + i0 < n0) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int i1 = I1s + 8 * grp + q;
+        if (i1 < n1) dst[(size_t)i1 * n0 + I0s + i0] = acc[q];
+      }
     }
     return;
   }
@@ -508,16 +563,19 @@ __global__ void __launch_bounds__(256) synthesis_kernel(SynArgs a, const float* 
   const int n0 = a.n0[0], n1 = a.n1[0];
   if (tile >= a.tiles[0]) return;
   const int ti0 = tile % a.tiles0[0], ti1 = tile / a.tiles0[0];
-  const int I0s = ti0 * ST0, I1s = ti1 * ST1;
-  float acc[2] = {0.f, 0.f};
-  for (int b = 0; b < kSaraWavelets; ++b) syn_basis(a, b, plane, coef, apx, I0s, I1s, sub, tlo, thi, acc);
-  const int li0 = threadIdx.x % ST0;
-  for (int r = 0; r < 2; ++r) {
-    const int i0 = I0s + li0, i1 = I1s + threadIdx.x / ST0 + 8 * r;
-    if (i0 < n0 && i1 < n1) {
-      const size_t o = (size_t)i1 * n0 + i0;
-      const float dirac = coef[(size_t)plane * a.s_stride + a.dirac_off + o];
-      out[(size_t)plane * a.out_stride + o] = a.alpha * (acc[r] + dirac);
+  const int I0s = ti0 * SY, I1s = ti1 * SX;
+#pragma unroll 1
+  for (int b = 0; b < kSaraWavelets; ++b) syn_dispatch(a, b, plane, coef, apx, I0s, I1s, S, acc);
+  if (I0s + i0 < n0) {
+    const float* dirac = coef + (size_t)plane * a.s_stride + a.dirac_off;
+    float* dst = out + (size_t)plane * a.out_stride;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int i1 = I1s + 8 * grp + q;
+      if (i1 < n1) {
+        const size_t o = (size_t)i1 * n0 + I0s + i0;
+        dst[o] = a.alpha * (acc[q] + dirac[o]);
+      }
     }
   }
 }
@@ -743,8 +801,8 @@ void sara_synthesis(const SaraPlan& p, const float* coef, float* out, float* apx
       a.m1[b] = p.n1[b][j];
       a.n0[b] = p.n0[b][j - 1];
       a.n1[b] = p.n1[b][j - 1];
-      a.tiles0[b] = ceil_div(a.n0[b], ST0);
-      a.tiles[b] = a.tiles0[b] * ceil_div(a.n1[b], ST1);
+      a.tiles0[b] = ceil_div(a.n0[b], SY);
+      a.tiles[b] = a.tiles0[b] * ceil_div(a.n1[b], SX);
       maxt = std::max(maxt, a.tiles[b]);
       a.a_off[b] = j == p.J ? p.offA[b] : p.apx_off[b][j];
       a.h_off[b] = p.offH[b][j];
