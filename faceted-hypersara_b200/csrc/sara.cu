@@ -434,25 +434,26 @@ struct SynArgs {
 };
 
 struct SynSmem {
-  float sub[4][SRX][SRYP];   // A, H, V, D coefficient windows
-  float tl[SRX][SY];         // y-filtered low  (A lo + H hi)
-  float th[SRX][SY];         // y-filtered high (V lo + D hi)
+  float sub[2][4][SRX][SRYP];  // A, H, V, D coefficient windows, double-buffered
+  float tl[SRX][SY];           // y-filtered low  (A lo + H hi)
+  float th[SRX][SY];           // y-filtered high (V lo + D hi)
 };
 
-// Adds basis b's synthesis of the tile at (I0s, I1s) to acc[q] (output row
-// threadIdx.x % 64, column 8 (threadIdx.x / 64) + q).
-template <int LF>
-__device__ __forceinline__ void syn_basis(const SynArgs& a, int b, int plane, const float* __restrict__ coef,
-                                          const float* __restrict__ apx, int I0s, int I1s, SynSmem& S,
-                                          float acc[8]) {
-  constexpr int H = LF / 2;
-  constexpr int RY = SY / 2 + H - 1, RX = SX / 2 + H - 1;
-  float lo[LF], hi[LF];
-#pragma unroll
-  for (int t = 0; t < LF; ++t) {
-    lo[t] = c_lo[b][t];
-    hi[t] = c_hi[b][t];
-  }
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 4 : 0;  // 0 source bytes: the destination is zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Starts the asynchronous copy of basis b's coefficient window for the tile
+// at (I0s, I1s) into buffer buf (zeros outside the coefficient arrays).
+__device__ __forceinline__ void syn_window(const SynArgs& a, int b, int plane, const float* __restrict__ coef,
+                                           const float* __restrict__ apx, int I0s, int I1s, SynSmem& S, int buf) {
+  const int H = b + 1;  // LF / 2
+  const int RY = SY / 2 + H - 1, RX = SX / 2 + H - 1;
   const int m0 = a.m0[b], m1 = a.m1[b];
   const int P0s = I0s / 2, P1s = I1s / 2;
   const float* A = (a.a_from_coef ? coef + (size_t)plane * a.s_stride : apx + (size_t)plane * a.apx_stride) +
@@ -462,28 +463,36 @@ __device__ __forceinline__ void syn_basis(const SynArgs& a, int b, int plane, co
   for (int idx = threadIdx.x; idx < RY * RX; idx += blockDim.x) {
     const int l1 = idx / RY, l0 = idx - l1 * RY;
     const int p0 = P0s + l0, p1 = P1s + l1;
-    float va = 0.f, vh = 0.f, vv = 0.f, vd = 0.f;
-    if (p0 < m0 && p1 < m1) {
-      const size_t o = (size_t)p1 * m0 + p0;
-      va = A[o];
-      vh = Hc[o];
-      vv = Hc[mm + o];
-      vd = Hc[2 * mm + o];
-    }
-    S.sub[0][l1][l0] = va;
-    S.sub[1][l1][l0] = vh;
-    S.sub[2][l1][l0] = vv;
-    S.sub[3][l1][l0] = vd;
+    const bool in = p0 < m0 && p1 < m1;
+    const size_t o = in ? (size_t)p1 * m0 + p0 : 0;
+    cp_async4(&S.sub[buf][0][l1][l0], A + o, in);
+    cp_async4(&S.sub[buf][1][l1][l0], Hc + o, in);
+    cp_async4(&S.sub[buf][2][l1][l0], Hc + mm + o, in);
+    cp_async4(&S.sub[buf][3][l1][l0], Hc + 2 * mm + o, in);
   }
-  __syncthreads();
+  cp_async_commit();
+}
+
+// Adds basis b's synthesis (window in buffer buf, already resident) to
+// acc[q] (output row threadIdx.x % 64, column 8 (threadIdx.x / 64) + q).
+template <int LF>
+__device__ __forceinline__ void syn_basis(int b, SynSmem& S, int buf, float acc[8]) {
+  constexpr int H = LF / 2;
+  constexpr int RX = SX / 2 + H - 1;
+  float lo[LF], hi[LF];
+#pragma unroll
+  for (int t = 0; t < LF; ++t) {
+    lo[t] = c_lo[b][t];
+    hi[t] = c_hi[b][t];
+  }
   // along y: task = (column l1, output pair k), k fastest
   for (int task = threadIdx.x; task < RX * (SY / 2); task += blockDim.x) {
     const int l1 = task / (SY / 2), k = task - l1 * (SY / 2);
     float le = 0.f, lo_ = 0.f, he = 0.f, ho = 0.f;
 #pragma unroll
     for (int j = 0; j < H; ++j) {
-      const float ca = S.sub[0][l1][k + j], ch = S.sub[1][l1][k + j];
-      const float cv = S.sub[2][l1][k + j], cd = S.sub[3][l1][k + j];
+      const float ca = S.sub[buf][0][l1][k + j], ch = S.sub[buf][1][l1][k + j];
+      const float cv = S.sub[buf][2][l1][k + j], cd = S.sub[buf][3][l1][k + j];
       le = fmaf(ca, lo[2 * j + 1], fmaf(ch, hi[2 * j + 1], le));
       lo_ = fmaf(ca, lo[2 * j], fmaf(ch, hi[2 * j], lo_));
       he = fmaf(cv, lo[2 * j + 1], fmaf(cd, hi[2 * j + 1], he));
@@ -512,30 +521,29 @@ __device__ __forceinline__ void syn_basis(const SynArgs& a, int b, int plane, co
     acc[2 * q] += e;
     acc[2 * q + 1] += o;
   }
-  // No barrier before the next basis: its window load rewrites sub, whose
-  // last reads (the y pass) precede this basis's second barrier, and its y
-  // pass rewrites tl/th only after its first barrier, which every thread
-  // reaches after finishing this x pass.
 }
 
-__device__ __forceinline__ void syn_dispatch(const SynArgs& a, int b, int plane, const float* __restrict__ coef,
-                                             const float* __restrict__ apx, int I0s, int I1s, SynSmem& S,
-                                             float acc[8]) {
+__device__ __forceinline__ void syn_dispatch(int b, SynSmem& S, int buf, float acc[8]) {
   switch (b) {
-    case 0: syn_basis<2>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    case 1: syn_basis<4>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    case 2: syn_basis<6>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    case 3: syn_basis<8>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    case 4: syn_basis<10>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    case 5: syn_basis<12>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    case 6: syn_basis<14>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
-    default: syn_basis<16>(a, b, plane, coef, apx, I0s, I1s, S, acc); break;
+    case 0: syn_basis<2>(b, S, buf, acc); break;
+    case 1: syn_basis<4>(b, S, buf, acc); break;
+    case 2: syn_basis<6>(b, S, buf, acc); break;
+    case 3: syn_basis<8>(b, S, buf, acc); break;
+    case 4: syn_basis<10>(b, S, buf, acc); break;
+    case 5: syn_basis<12>(b, S, buf, acc); break;
+    case 6: syn_basis<14>(b, S, buf, acc); break;
+    default: syn_basis<16>(b, S, buf, acc); break;
   }
 }
 
-__global__ void __launch_bounds__(256, 3) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
+// Final level: the window of basis b+1 is in flight while basis b is filtered.
+// Buffer (b+1)&1 was last read by basis b-1's y pass, which every thread has
+// finished at basis b-1's second barrier; tl/th are rewritten by basis b's y
+// pass only after its first barrier, which follows basis b-1's x pass.
+__global__ void __launch_bounds__(256) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
                                                         float* __restrict__ apx, float* __restrict__ out) {
-  __shared__ SynSmem S;
+  extern __shared__ __align__(16) unsigned char syn_smem[];
+  SynSmem& S = *reinterpret_cast<SynSmem*>(syn_smem);
   const int plane = blockIdx.z;
   const int tile = blockIdx.x;
   const int i0 = threadIdx.x % SY, grp = threadIdx.x / SY;
@@ -547,7 +555,10 @@ __global__ void __launch_bounds__(256, 3) synthesis_kernel(SynArgs a, const floa
     if (tile >= a.tiles[b]) return;
     const int ti0 = tile % a.tiles0[b], ti1 = tile / a.tiles0[b];
     const int I0s = ti0 * SY, I1s = ti1 * SX;
-    syn_dispatch(a, b, plane, coef, apx, I0s, I1s, S, acc);
+    syn_window(a, b, plane, coef, apx, I0s, I1s, S, 0);
+    cp_async_wait<0>();
+    __syncthreads();
+    syn_dispatch(b, S, 0, acc);
     const int n0 = a.n0[b], n1 = a.n1[b];
     float* dst = apx + (size_t)plane * a.apx_stride + a.out_off[b];
     if (I0s + i0 < n0) {
@@ -564,8 +575,18 @@ __global__ void __launch_bounds__(256, 3) synthesis_kernel(SynArgs a, const floa
   if (tile >= a.tiles[0]) return;
   const int ti0 = tile % a.tiles0[0], ti1 = tile / a.tiles0[0];
   const int I0s = ti0 * SY, I1s = ti1 * SX;
+  syn_window(a, 0, plane, coef, apx, I0s, I1s, S, 0);
 #pragma unroll 1
-  for (int b = 0; b < kSaraWavelets; ++b) syn_dispatch(a, b, plane, coef, apx, I0s, I1s, S, acc);
+  for (int b = 0; b < kSaraWavelets; ++b) {
+    if (b + 1 < kSaraWavelets) {
+      syn_window(a, b + 1, plane, coef, apx, I0s, I1s, S, (b + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    syn_dispatch(b, S, b & 1, acc);
+  }
   if (I0s + i0 < n0) {
     const float* dirac = coef + (size_t)plane * a.s_stride + a.dirac_off;
     float* dst = out + (size_t)plane * a.out_stride;
@@ -793,6 +814,14 @@ void sara_dirac(const SaraPlan& p, const float* x, float* coef, int np, cudaStre
 void sara_synthesis(const SaraPlan& p, const float* coef, float* out, float* apx, int np, float alpha,
                     cudaStream_t s) {
   upload_filters();
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr[dev]) {
+    FHS_CUDA(cudaFuncSetAttribute(synthesis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(SynSmem)));
+    attr[dev] = true;
+  }
   for (int j = p.J; j >= 1; --j) {
     SynArgs a{};
     int maxt = 0;
@@ -816,7 +845,7 @@ void sara_synthesis(const SaraPlan& p, const float* coef, float* out, float* apx
     a.dirac_off = p.boff[kSaraWavelets];
     a.alpha = alpha / 3.f;
     dim3 grid(a.final_level ? a.tiles[0] : maxt, a.final_level ? 1 : kSaraWavelets, np);
-    synthesis_kernel<<<grid, 256, 0, s>>>(a, coef, apx, out);
+    synthesis_kernel<<<grid, 256, sizeof(SynSmem), s>>>(a, coef, apx, out);
     count_launch();
     FHS_LAUNCH_CHECK();
   }
