@@ -225,6 +225,7 @@ __global__ void __launch_bounds__(256) analysis_kernel(LevelArgs a, const float*
 // basis index selects the instantiation) so the x-filter stays in registers.
 constexpr int APH = (2 * AT0 + kSaraMaxFilter - 2 + 1) / 2;  // 39 rows per parity
 constexpr int kApChunk = 16;                                 // channels staged per phase
+constexpr int kApBand = 256;                                 // tiles per basis-major band of the grid
 
 template <int MAXL, int LF, bool LAST>
 __device__ __forceinline__ void analysis_prox_body(const LevelArgs& a, int b, int tile, int g,
@@ -361,7 +362,12 @@ __global__ void __launch_bounds__(256, (MAXL > 16 ? 1 : 2)) analysis_prox_kernel
                                                             double* __restrict__ l21_acc) {
   extern __shared__ float sm_ap[];
   __shared__ double red[8];
-  const int b = blockIdx.x, tile = blockIdx.y, g = blockIdx.z;
+  // blockIdx.x = (band, basis, tile in band): the CTAs resident together run
+  // one basis (one code path), and the 8 bases of a band of kApBand tiles
+  // follow each other while its input is still in L2
+  const int band = blockIdx.x / (kSaraWavelets * kApBand);
+  const int rem = blockIdx.x - band * (kSaraWavelets * kApBand);
+  const int b = rem / kApBand, tile = band * kApBand + rem % kApBand, g = blockIdx.y;
   if (tile >= a.tiles[b]) return;
   if (a.last) {
     switch (b) {
@@ -460,15 +466,18 @@ __device__ __forceinline__ void syn_window(const SynArgs& a, int b, int plane, c
                    a.a_off[b];
   const float* Hc = coef + (size_t)plane * a.s_stride + a.h_off[b];
   const size_t mm = (size_t)m0 * m1;
-  for (int idx = threadIdx.x; idx < RY * RX; idx += blockDim.x) {
-    const int l1 = idx / RY, l0 = idx - l1 * RY;
-    const int p0 = P0s + l0, p1 = P1s + l1;
-    const bool in = p0 < m0 && p1 < m1;
-    const size_t o = in ? (size_t)p1 * m0 + p0 : 0;
-    cp_async4(&S.sub[buf][0][l1][l0], A + o, in);
-    cp_async4(&S.sub[buf][1][l1][l0], Hc + o, in);
-    cp_async4(&S.sub[buf][2][l1][l0], Hc + mm + o, in);
-    cp_async4(&S.sub[buf][3][l1][l0], Hc + 2 * mm + o, in);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int l1 = warp; l1 < RX; l1 += 8) {  // one window column per warp, rows across lanes
+    const int p1 = P1s + l1;
+    for (int l0 = lane; l0 < RY; l0 += 32) {
+      const int p0 = P0s + l0;
+      const bool in = p0 < m0 && p1 < m1;
+      const size_t o = in ? (size_t)p1 * m0 + p0 : 0;
+      cp_async4(&S.sub[buf][0][l1][l0], A + o, in);
+      cp_async4(&S.sub[buf][1][l1][l0], Hc + o, in);
+      cp_async4(&S.sub[buf][2][l1][l0], Hc + mm + o, in);
+      cp_async4(&S.sub[buf][3][l1][l0], Hc + 2 * mm + o, in);
+    }
   }
   cp_async_commit();
 }
@@ -602,7 +611,9 @@ __global__ void __launch_bounds__(256) synthesis_kernel(SynArgs a, const float* 
 }
 
 // ------------------------------------------------------------- prox
-template <int MAXL>
+// DIRAC: every row lies in the Dirac part (coefficients xhat/3, no branch, so
+// the loads of all channels issue together).
+template <int MAXL, bool DIRAC>
 __global__ void __launch_bounds__(256) l21_prox_kernel(float* __restrict__ v1, const float* __restrict__ coef,
                                                        const float* __restrict__ xhat,
                                                        const float* __restrict__ weights,
@@ -622,7 +633,8 @@ __global__ void __launch_bounds__(256) l21_prox_kernel(float* __restrict__ v1, c
     for (int l = 0; l < MAXL; ++l) {
       if (l < lg) {
         const size_t plane = (size_t)g * lg + l;
-        const float c = i < dirac_off ? coef[plane * s + i] : xhat[plane * npix + (i - dirac_off)] * (1.f / 3.f);
+        const float c = (DIRAC || i >= dirac_off) ? xhat[plane * npix + (i - dirac_off)] * (1.f / 3.f)
+                                                  : coef[plane * s + i];
         w[l] = v1[plane * s + i] + c;
         ss = fmaf(w[l], w[l], ss);
       }
@@ -766,7 +778,7 @@ void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* 
     a.first = j == 1;
     a.last = j == p.J;
     a.in_scale = j == 1 ? 1.f / 3.f : 1.f;
-    dim3 grid(kSaraWavelets, maxt, n_groups);
+    dim3 grid(ceil_div(maxt, kApBand) * kSaraWavelets * kApBand, n_groups);
 #define FHS_AP(MAXL) launch_analysis_prox<MAXL>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc)
     if (lg <= 1)
       FHS_AP(1);
@@ -787,7 +799,7 @@ void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* 
   const int64_t off = p.boff[kSaraWavelets];
   dim3 grid(nblk(npix), n_groups);
 #define FHS_DP(MAXL)                                                                                            \
-  l21_prox_kernel<MAXL><<<grid, 256, 0, s>>>(v1, nullptr, xhat, weights, beta, p.s, off, npix, lg, nullptr, off, \
+  l21_prox_kernel<MAXL, true><<<grid, 256, 0, s>>>(v1, nullptr, xhat, weights, beta, p.s, off, npix, lg, nullptr, off, \
                                              l21_acc)
   if (lg <= 1)
     FHS_DP(1);
@@ -857,7 +869,7 @@ void sara_l21_prox(const SaraPlan& p, float* v1, const float* coef, const float*
   dim3 grid(nblk(p.s), n_groups);
   const int64_t off = p.boff[kSaraWavelets];
 #define FHS_L21(MAXL)                                                                                       \
-  l21_prox_kernel<MAXL><<<grid, 256, 0, s>>>(v1, coef, xhat, weights, beta, p.s, off, npix, lg, l21_partials, 0, \
+  l21_prox_kernel<MAXL, false><<<grid, 256, 0, s>>>(v1, coef, xhat, weights, beta, p.s, off, npix, lg, l21_partials, 0, \
                                              nullptr)
   if (lg <= 1)
     FHS_L21(1);
