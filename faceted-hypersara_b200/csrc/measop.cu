@@ -649,6 +649,33 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
     h.geom[p] = g[m];
     h.perm[p] = (int32_t)m;
   }
+  // Inside each sub-bin, deal the visibilities round-robin over the 16
+  // classes (start row mod 8, start column mod 2): the degridding threads of a
+  // half-warp then read their taps' grid values (float2, column pitch 72) from
+  // 16 distinct bank pairs in the dense sub-bins.
+  std::vector<float4> tg;
+  std::vector<int32_t> tp, order;
+  for (int k = 0; k < op->nkeys; ++k) {
+    const int a = h.sb_off[k], b = h.sb_off[k + 1];
+    if (b - a < 2) continue;
+    int cnt[16] = {0};
+    order.assign(b - a, 0);
+    for (int i = a; i < b; ++i) {
+      unsigned kp;
+      std::memcpy(&kp, &h.geom[i].z, sizeof(kp));
+      const int c = (int)(kp & 7u) + 8 * (int)((kp >> 14) & 1u);
+      order[i - a] = cnt[c]++ * 16 + c;  // (rank within its class, class)
+    }
+    std::vector<int32_t> idx(b - a);
+    for (int i = 0; i < b - a; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](int u, int v) { return order[u] < order[v]; });
+    tg.assign(h.geom.begin() + a, h.geom.begin() + b);
+    tp.assign(h.perm.begin() + a, h.perm.begin() + b);
+    for (int i = 0; i < b - a; ++i) {
+      h.geom[a + i] = tg[idx[i]];
+      h.perm[a + i] = tp[idx[i]];
+    }
+  }
   h.set = true;
 }
 
