@@ -38,7 +38,6 @@ unsigned long long g_launches = 0;
 
 namespace {
 
-constexpr int kS = kTableSamples;
 constexpr int kSmemPitch = kTileCells + kBinCells;  // 72 (>= 64 + J - 1)
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -113,8 +112,23 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
   }
   __syncthreads();
   const int64_t vo = op.ch_voff[ch];
+  // software pipeline: the next visibility's geometry and dual operands are
+  // loaded while this one is interpolated
+  float4 gm_n = make_float4(0.f, 0.f, 0.f, 0.f);
+  float2 yv_n = make_float2(0.f, 0.f), vv_n = yv_n, go_n = yv_n;
+  auto fetch = [&](int i) {
+    gm_n = __ldg(op.geom + vo + i);
+    if (DUAL) {
+      yv_n = y[vo + i];
+      vv_n = v2[vo + i];
+      go_n = gold[vo + i];
+    }
+  };
+  if (beg + (int)threadIdx.x < end) fetch(beg + threadIdx.x);
   for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
-    const float4 gm = __ldg(op.geom + vo + i);
+    const float4 gm = gm_n;
+    const float2 yv = yv_n, vv = vv_n, go = go_n;
+    if (i + (int)blockDim.x < end) fetch(i + blockDim.x);
     const unsigned kp = __float_as_uint(gm.z);
     const int d0 = (int)(kp & 0x3FFFu) - a0;
     const int d1 = (int)((kp >> 14) & 0x3FFFu) - a1;
@@ -134,9 +148,6 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
     if (!DUAL) {
       out[vo + i] = gfx;
     } else {
-      const float2 yv = y[vo + i];
-      const float2 vv = v2[vo + i];
-      const float2 go = gold[vo + i];
       const float2 r = make_float2(gfx.x - yv.x, gfx.y - yv.y);
       const int blk = (int)(kp >> 28);
       double n0;
@@ -336,26 +347,52 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
         sd[lane] = make_int2(d0, d1 - xb);
       }
       __syncwarp();
-      for (int k = 0; k < n; ++k) {
-        const int2 d = sd[k];                 // (row offset, band column offset)
-        const float2* sk = st + k * 2 * J;
-        const int a = d.y * kAccPitch + d.x;  // accumulator index of tap (0, 0)
-        const int tc = d.y + xb;              // tile column of tap (0, 0)
-        if ((unsigned)(d.x + jyA) < (unsigned)T0 && (unsigned)(tc + jxA) < (unsigned)T1) {
-          const float2 val = cmul(sk[jyA], sk[J + jxA]);
-          float2 o = ab[a + offA];
-          o.x += val.x;
-          o.y += val.y;
-          ab[a + offA] = o;
+      // Taps outside the tile need no test: columns left of the tile (band 0)
+      // or right of it (band 8, columns 8-13) land in band columns the final
+      // sum ignores, and own rows stay below 64 + 7 <= kAccPitch.  Only the
+      // ring above the tile (part 1) reaches negative rows, which are skipped.
+      if (part == 0) {
+        for (int k = 0; k < n; ++k) {
+          const int2 d = sd[k];                 // (row offset, band column offset)
+          const float2* sk = st + k * 2 * J;
+          const int a = d.y * kAccPitch + d.x;  // accumulator index of tap (0, 0)
+          {
+            const float2 val = cmul(sk[jyA], sk[J + jxA]);
+            float2 o = ab[a + offA];
+            o.x += val.x;
+            o.y += val.y;
+            ab[a + offA] = o;
+          }
+          if (hasB) {
+            const float2 val = cmul(sk[jyB], sk[J + jxB]);
+            float2 o = ab[a + offB];
+            o.x += val.x;
+            o.y += val.y;
+            ab[a + offB] = o;
+          }
+          __syncwarp();
         }
-        if (hasB && (unsigned)(d.x + jyB) < (unsigned)T0 && (unsigned)(tc + jxB) < (unsigned)T1) {
-          const float2 val = cmul(sk[jyB], sk[J + jxB]);
-          float2 o = ab[a + offB];
-          o.x += val.x;
-          o.y += val.y;
-          ab[a + offB] = o;
+      } else {
+        for (int k = 0; k < n; ++k) {
+          const int2 d = sd[k];
+          const float2* sk = st + k * 2 * J;
+          const int a = d.y * kAccPitch + d.x;
+          if (d.x + jyA >= 0) {
+            const float2 val = cmul(sk[jyA], sk[J + jxA]);
+            float2 o = ab[a + offA];
+            o.x += val.x;
+            o.y += val.y;
+            ab[a + offA] = o;
+          }
+          if (hasB && d.x + jyB >= 0) {
+            const float2 val = cmul(sk[jyB], sk[J + jxB]);
+            float2 o = ab[a + offB];
+            o.x += val.x;
+            o.y += val.y;
+            ab[a + offB] = o;
+          }
+          __syncwarp();
         }
-        __syncwarp();
       }
     }
   }
