@@ -76,7 +76,9 @@ __device__ __forceinline__ int wrap(int k, int K) {
 // MODE 0: out = G Fx.  MODE 1: l2-ball dual, pass 1.  MODE 2: ellipsoid dual,
 // pass 1 (d = v2/pU + 2 GFx - gold - y to zbuf, block norms of the first FB
 // point t_1 - y = w0 + (mu/pU)(d - w0), w0 = proj - y).
-template <int J, int MODE>
+// NB: blocks per channel the per-thread FP64 norm accumulators cover (dual
+// modes; shared-memory FP64 atomics per visibility would serialise the warp).
+template <int J, int MODE, int NB>
 __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid,
                                                      const WorkItem* __restrict__ items,
                                                      const int* __restrict__ order, int item0,
@@ -111,6 +113,9 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
     sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * op.Ky + k0);
   }
   __syncthreads();
+  double nacc[NB][2];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) nacc[b][0] = nacc[b][1] = 0.0;
   const int64_t vo = op.ch_voff[ch];
   // software pipeline: the next visibility's geometry and dual operands are
   // loaded while this one is interpolated
@@ -166,11 +171,28 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
         n0 = tx * tx + ty * ty;
       }
       gold[vo + i] = gfx;
-      atomicAdd(&bacc[2 * blk], n0);
-      atomicAdd(&bacc[2 * blk + 1], (double)r.x * r.x + (double)r.y * r.y);
+      const double n1 = (double)r.x * r.x + (double)r.y * r.y;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        if (b == blk) {
+          nacc[b][0] += n0;
+          nacc[b][1] += n1;
+        }
+      }
     }
   }
   if (DUAL) {
+    // warp sums, then one shared atomic per warp and value
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        double v = nacc[b][f];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&bacc[2 * b + f], v);
+      }
+    }
     __syncthreads();
     if (threadIdx.x < kMaxBlocksPerChannel * 2)
       partials[(size_t)it.slot * kMaxBlocksPerChannel * 2 + threadIdx.x] = bacc[threadIdx.x];
@@ -909,8 +931,8 @@ PrecondView MeasOp::precond_view(const double2* w) const {
 void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s) {
   const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
   if (n == 0) return;
-  degrid_kernel<7, 0><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, out, nullptr,
-                                        nullptr, nullptr, nullptr, nullptr, PrecondView{});
+  degrid_kernel<7, 0, 1><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, out, nullptr,
+                                           nullptr, nullptr, nullptr, nullptr, PrecondView{});
   count_launch();
   FHS_LAUNCH_CHECK();
 }
@@ -927,25 +949,46 @@ void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, 
   FHS_LAUNCH_CHECK();
 }
 
-void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
-                        cudaStream_t s) {
-  const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
-  if (n == 0) return;
-  degrid_kernel<7, 1><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, nullptr, v2, gold,
-                                        y, op->partials.p, op->zbuf.p, PrecondView{});
+template <int MODE, int NB>
+static void degrid_dual(const MeasOp* op, int i0, int n, const float2* v2, float2* gold, const float2* y,
+                        PrecondView pc, cudaStream_t s) {
+  degrid_kernel<7, MODE, NB><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, nullptr, v2,
+                                               gold, y, op->partials.p, op->zbuf.p, pc);
   count_launch();
   FHS_LAUNCH_CHECK();
+}
+
+// the fewest per-thread block accumulators that cover every channel
+template <int MODE>
+static void degrid_dual_nb(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold, const float2* y,
+                           PrecondView pc, cudaStream_t s) {
+  const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
+  if (n == 0) return;
+  int nb = 1;
+  for (int c = c0; c < c0 + nc; ++c) nb = std::max(nb, (int)op->h_nblk[c]);
+  if (nb <= 1)
+    degrid_dual<MODE, 1>(op, i0, n, v2, gold, y, pc, s);
+  else if (nb <= 2)
+    degrid_dual<MODE, 2>(op, i0, n, v2, gold, y, pc, s);
+  else if (nb <= 4)
+    degrid_dual<MODE, 4>(op, i0, n, v2, gold, y, pc, s);
+  else if (nb <= 6)
+    degrid_dual<MODE, 6>(op, i0, n, v2, gold, y, pc, s);
+  else if (nb <= 8)
+    degrid_dual<MODE, 8>(op, i0, n, v2, gold, y, pc, s);
+  else
+    degrid_dual<MODE, 16>(op, i0, n, v2, gold, y, pc, s);
+}
+
+void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
+                        cudaStream_t s) {
+  degrid_dual_nb<1>(op, c0, nc, v2, gold, y, PrecondView{}, s);
 }
 
 void launch_degrid_dual_precond(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold,
                                 const float2* y, const double2* w, cudaStream_t s) {
   FHS_CHECK(op->precond, FHS_ERR_STATE, "no preconditioner set");
-  const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
-  if (n == 0) return;
-  degrid_kernel<7, 2><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, nullptr, v2, gold,
-                                        y, op->partials.p, op->zbuf.p, op->precond_view(w));
-  count_launch();
-  FHS_LAUNCH_CHECK();
+  degrid_dual_nb<2>(op, c0, nc, v2, gold, y, op->precond_view(w), s);
 }
 
 static void block_reduce(const MeasOp* op, int c0, int nc, int mode, cudaStream_t s) {
