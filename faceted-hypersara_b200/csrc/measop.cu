@@ -78,7 +78,9 @@ __device__ __forceinline__ int wrap(int k, int K) {
 // point t_1 - y = w0 + (mu/pU)(d - w0), w0 = proj - y).
 // NB: blocks per channel the per-thread FP64 norm accumulators cover (dual
 // modes; shared-memory FP64 atomics per visibility would serialise the warp).
-template <int J, int MODE, int NB>
+// HALF: the grid is the half spectrum of a real-to-complex FFT,
+// [Kx][Ky/2 + 1] per channel; G(k0, k1) for k0 > Ky/2 is conj(G(-k0, -k1)).
+template <int J, int MODE, int NB, bool HALF>
 __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid,
                                                      const WorkItem* __restrict__ items,
                                                      const int* __restrict__ order, int item0,
@@ -106,11 +108,19 @@ __global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __
     if (threadIdx.x < kMaxBlocksPerChannel * 2) bacc[threadIdx.x] = 0.0;
   }
   const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
-  const float2* g = grid + (size_t)ch * op.Ky * op.Kx;
+  const int Kh = op.Ky / 2 + 1;
+  const float2* g = grid + (size_t)ch * (HALF ? Kh : op.Ky) * op.Kx;
   for (int idx = threadIdx.x; idx < R * R; idx += blockDim.x) {
     const int c1 = idx / R, cc0 = idx - c1 * R;
     const int k0 = wrap(a0 + cc0, op.Ky), k1 = wrap(a1 + c1, op.Kx);
-    sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * op.Ky + k0);
+    if (!HALF) {
+      sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * op.Ky + k0);
+    } else if (k0 < Kh) {
+      sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * Kh + k0);
+    } else {  // Hermitian mirror
+      const float2 m = __ldg(g + (size_t)(k1 == 0 ? 0 : op.Kx - k1) * Kh + (op.Ky - k0));
+      sm[c1 * P + cc0] = make_float2(m.x, -m.y);
+    }
   }
   __syncthreads();
   double nacc[NB][2];
@@ -605,6 +615,7 @@ MeasOp::~MeasOp() {
   DeviceGuard g(device);
   if (plan_all) cufftDestroy(plan_all);
   if (plan_one) cufftDestroy(plan_one);
+  if (plan_r2c) cufftDestroy(plan_r2c);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -893,6 +904,46 @@ void measop_commit(MeasOp* op) {
   op->committed = true;
 }
 
+__global__ void pad_real_kernel(const float* __restrict__ x, float* __restrict__ pad, const float* __restrict__ sy,
+                                const float* __restrict__ sx, int Ny, int Nx, int Ky, int Kx, int p0) {
+  const int64_t N = (int64_t)Ny * Nx;
+  const int plane = blockIdx.y;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(p / Ny), iy = (int)(p - (int64_t)ix * Ny);
+    int ky = iy - Ny / 2;
+    ky += ky < 0 ? Ky : 0;
+    int kx = ix - Nx / 2;
+    kx += kx < 0 ? Kx : 0;
+    pad[(size_t)(p0 + plane) * Ky * Kx + (size_t)kx * Ky + ky] = x[(size_t)plane * N + p] * sy[iy] * sx[ix];
+  }
+}
+
+void measop_enable_r2c(MeasOp* op) {
+  if (op->plan_r2c) return;
+  DeviceGuard g(op->device);
+  cudaStream_t s = op->stream;
+  op->padr.alloc((size_t)op->L * op->No());
+  op->padr.zero(s);
+  int n[2] = {op->Kx, op->Ky};
+  FHS_CUFFT(cufftPlanMany(&op->plan_r2c, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, op->L));
+  FHS_CUFFT(cufftSetStream(op->plan_r2c, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s) {
+  FHS_CHECK(op->plan_r2c, FHS_ERR_STATE, "real-to-complex path not enabled");
+  dim3 grid(grid_blocks(op->Npix(), 256), np);
+  pad_real_kernel<<<grid, 256, 0, s>>>(x, op->padr.p, op->sy.p, op->sx.p, op->Ny, op->Nx, op->Ky, op->Kx, p0);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+}
+
+void fft_forward_r2c(const MeasOp* op, cudaStream_t s) {
+  (void)s;
+  FHS_CHECK(op->plan_r2c, FHS_ERR_STATE, "real-to-complex path not enabled");
+  FHS_CUFFT(cufftExecR2C(op->plan_r2c, op->padr.p, (cufftComplex*)op->gridA.p));
+}
+
 void launch_pad(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s) {
   dim3 grid(grid_blocks(op->Npix(), 256), np);
   pad_kernel<<<grid, 256, 0, s>>>(x, op->pad.p, op->sy.p, op->sx.p, op->Ny, op->Nx, op->Ky, op->Kx, p0);
@@ -928,11 +979,15 @@ PrecondView MeasOp::precond_view(const double2* w) const {
   return v;
 }
 
-void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s) {
+void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s, bool half) {
   const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
   if (n == 0) return;
-  degrid_kernel<7, 0, 1><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, out, nullptr,
-                                           nullptr, nullptr, nullptr, nullptr, PrecondView{});
+  if (half)
+    degrid_kernel<7, 0, 1, true><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, out,
+                                                   nullptr, nullptr, nullptr, nullptr, nullptr, PrecondView{});
+  else
+    degrid_kernel<7, 0, 1, false><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, out,
+                                                    nullptr, nullptr, nullptr, nullptr, nullptr, PrecondView{});
   count_launch();
   FHS_LAUNCH_CHECK();
 }
@@ -951,9 +1006,13 @@ void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, 
 
 template <int MODE, int NB>
 static void degrid_dual(const MeasOp* op, int i0, int n, const float2* v2, float2* gold, const float2* y,
-                        PrecondView pc, cudaStream_t s) {
-  degrid_kernel<7, MODE, NB><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0, nullptr, v2,
-                                               gold, y, op->partials.p, op->zbuf.p, pc);
+                        PrecondView pc, cudaStream_t s, bool half) {
+  if (half)
+    degrid_kernel<7, MODE, NB, true><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0,
+                                                       nullptr, v2, gold, y, op->partials.p, op->zbuf.p, pc);
+  else
+    degrid_kernel<7, MODE, NB, false><<<n, 256, 0, s>>>(op->view(), op->gridA.p, op->dg_items.p, nullptr, i0,
+                                                        nullptr, v2, gold, y, op->partials.p, op->zbuf.p, pc);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
@@ -961,34 +1020,34 @@ static void degrid_dual(const MeasOp* op, int i0, int n, const float2* v2, float
 // the fewest per-thread block accumulators that cover every channel
 template <int MODE>
 static void degrid_dual_nb(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold, const float2* y,
-                           PrecondView pc, cudaStream_t s) {
+                           PrecondView pc, cudaStream_t s, bool half) {
   const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
   if (n == 0) return;
   int nb = 1;
   for (int c = c0; c < c0 + nc; ++c) nb = std::max(nb, (int)op->h_nblk[c]);
   if (nb <= 1)
-    degrid_dual<MODE, 1>(op, i0, n, v2, gold, y, pc, s);
+    degrid_dual<MODE, 1>(op, i0, n, v2, gold, y, pc, s, half);
   else if (nb <= 2)
-    degrid_dual<MODE, 2>(op, i0, n, v2, gold, y, pc, s);
+    degrid_dual<MODE, 2>(op, i0, n, v2, gold, y, pc, s, half);
   else if (nb <= 4)
-    degrid_dual<MODE, 4>(op, i0, n, v2, gold, y, pc, s);
+    degrid_dual<MODE, 4>(op, i0, n, v2, gold, y, pc, s, half);
   else if (nb <= 6)
-    degrid_dual<MODE, 6>(op, i0, n, v2, gold, y, pc, s);
+    degrid_dual<MODE, 6>(op, i0, n, v2, gold, y, pc, s, half);
   else if (nb <= 8)
-    degrid_dual<MODE, 8>(op, i0, n, v2, gold, y, pc, s);
+    degrid_dual<MODE, 8>(op, i0, n, v2, gold, y, pc, s, half);
   else
-    degrid_dual<MODE, 16>(op, i0, n, v2, gold, y, pc, s);
+    degrid_dual<MODE, 16>(op, i0, n, v2, gold, y, pc, s, half);
 }
 
 void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
-                        cudaStream_t s) {
-  degrid_dual_nb<1>(op, c0, nc, v2, gold, y, PrecondView{}, s);
+                        cudaStream_t s, bool half) {
+  degrid_dual_nb<1>(op, c0, nc, v2, gold, y, PrecondView{}, s, half);
 }
 
 void launch_degrid_dual_precond(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold,
-                                const float2* y, const double2* w, cudaStream_t s) {
+                                const float2* y, const double2* w, cudaStream_t s, bool half) {
   FHS_CHECK(op->precond, FHS_ERR_STATE, "no preconditioner set");
-  degrid_dual_nb<2>(op, c0, nc, v2, gold, y, op->precond_view(w), s);
+  degrid_dual_nb<2>(op, c0, nc, v2, gold, y, op->precond_view(w), s, half);
 }
 
 static void block_reduce(const MeasOp* op, int c0, int nc, int mode, cudaStream_t s) {

@@ -91,6 +91,10 @@ struct MeasOp {
   // output), B (gridding output, IFFT input).  [L][Kx][Ky] each.
   DevBuf<float2> pad, gridA, gridB;
   cufftHandle plan_all = 0, plan_one = 0;
+  // real-to-complex forward path of the solvers (measop_enable_r2c): the
+  // padded real image and its half spectrum (in gridA, [L][Kx][Ky/2 + 1])
+  DevBuf<float> padr;
+  cufftHandle plan_r2c = 0;
 
   // scratch for API-level calls
   DevBuf<float2> vis_a, vis_b;
@@ -143,15 +147,21 @@ void launch_pad(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s
 // FFT of pad planes -> gridA (forward), or gridB -> gridA (inverse)
 void fft_forward(const MeasOp* op, int p0, int np, cudaStream_t s);
 void fft_inverse(const MeasOp* op, int p0, int np, cudaStream_t s);
-// GFx for channels [c0, c0+nc) from gridA into out (sorted visibility order)
-void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s);
+// GFx for channels [c0, c0+nc) from gridA into out (sorted visibility order);
+// half: gridA holds the half spectrum of fft_forward_r2c
+void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s, bool half = false);
+// real-to-complex forward path: padr <- s .* x (all planes placed as launch_pad),
+// gridA <- half spectrum of padr (all L planes)
+void measop_enable_r2c(MeasOp* op);
+void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s);
+void fft_forward_r2c(const MeasOp* op, cudaStream_t s);
 // gridB <- G^H v (v sorted, channels [c0, c0+nc)); non-empty tiles only
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
 // out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1
 void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s);
 // fused dual update, pass 1: GFx, z = v2 + 2 GFx - gold - y -> zbuf, GFx -> gold, block partials
 void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
-                        cudaStream_t s);
+                        cudaStream_t s, bool half = false);
 // block reduction: scale = 1 - min(eps/||z||, 1); stats for the report
 void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s);
 // fused dual update, pass 2: v2 <- zbuf*scale, gridB <- G^H v2
@@ -162,7 +172,7 @@ void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t
 void measop_set_preconditioner(MeasOp* op, int channel, const double* pu);
 // pass 1: d = v2/pU + 2 GFx - gold - y -> zbuf, GFx -> gold, ||t_1 - y||^2 partials
 void launch_degrid_dual_precond(const MeasOp* op, int c0, int nc, const float2* v2, float2* gold,
-                                const float2* y, const double2* w, cudaStream_t s);
+                                const float2* y, const double2* w, cudaStream_t s, bool half = false);
 // block norms -> scale of the first projection, FB counters reset
 void launch_block_reduce_precond(const MeasOp* op, int c0, int nc, cudaStream_t s);
 // max_itr forward-backward passes (finished blocks skip their visibilities)

@@ -49,7 +49,7 @@ __device__ __forceinline__ void block_sum2(double& a, double& b) {
 }
 
 __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, const float* __restrict__ g,
-                                                         float* __restrict__ xhat, float2* __restrict__ pad,
+                                                         float* __restrict__ xhat, float* __restrict__ pad,
                                                          const float* __restrict__ sy, const float* __restrict__ sx,
                                                          int Ny, int Nx, int Ky, int Kx, double* __restrict__ part) {
   const int plane = blockIdx.y;
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, 
   float* xp = x + (size_t)plane * N;
   const float* gp = g + (size_t)plane * N;
   float* hp = xhat + (size_t)plane * N;
-  float2* pp = pad + (size_t)plane * Ky * Kx;
+  float* pp = pad + (size_t)plane * Ky * Kx;
   double a = 0.0, b = 0.0;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
     const float xo = xp[p];
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, 
     ky += ky < 0 ? Ky : 0;
     int kx = ix - Nx / 2;
     kx += kx < 0 ? Kx : 0;
-    pp[(size_t)kx * Ky + ky] = make_float2(xn * sy[iy] * sx[ix], 0.f);
+    pp[(size_t)kx * Ky + ky] = xn * sy[iy] * sx[ix];
   }
   block_sum2(a, b);
   if (threadIdx.x == 0) {
@@ -239,15 +239,15 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
     ++stage;
   };
   mark();
-  primal_pad_kernel<<<dim3(kPrimalBlocks, L), 256, 0, s>>>(S->x.p, S->g.p, S->xhat.p, op->pad.p, op->sy.p, op->sx.p,
-                                                           S->Ny, S->Nx, op->Ky, op->Kx, S->primal_part.p);
+  primal_pad_kernel<<<dim3(kPrimalBlocks, L), 256, 0, s>>>(S->x.p, S->g.p, S->xhat.p, op->padr.p, op->sy.p,
+                                                           op->sx.p, S->Ny, S->Nx, op->Ky, op->Kx, S->primal_part.p);
   count_launch();
   FHS_LAUNCH_CHECK();
   mark();
-  fft_forward(op, 0, L, s);
+  fft_forward_r2c(op, s);
   mark();
   if (S->precond) {
-    launch_degrid_dual_precond(op, 0, L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s);
+    launch_degrid_dual_precond(op, 0, L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s, true);
     mark();
     launch_block_reduce_precond(op, 0, L, s);
     mark();
@@ -256,7 +256,7 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
     launch_grid_dual_precond(op, 0, L, S->v2.p, S->projw.p, s);
     mark();
   } else {
-    launch_degrid_dual(op, 0, L, S->v2.p, S->gold.p, S->y.p, s);
+    launch_degrid_dual(op, 0, L, S->v2.p, S->gold.p, S->y.p, s, true);
     mark();
     launch_block_reduce(op, 0, L, s);
     mark();
@@ -413,6 +413,7 @@ fhs_status fhs_solver_create(fhs_measop* op_, const fhs_solver_config* cfg, fhs_
       S->nuclear = true;
     }
     S->sp = sara_plan(S->Ny, S->Nx, S->nlevel);
+    measop_enable_r2c(op);
     if (S->nuclear) {
       int Qy = 1, Qx = 1, oy = 0, ox = 0, win = FHS_WINDOW_NONE;
       std::vector<int> sy, sx;
@@ -593,9 +594,9 @@ fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
     if (S->nuclear) S->v0.zero(s);
     S->ring_counter.zero(s);
     // Fx_old: keep G A x_init per visibility (linearity of G)
-    launch_pad(op, S->x.p, 0, S->L, s);
-    fft_forward(op, 0, S->L, s);
-    launch_degrid_plain(op, 0, S->L, S->gold.p, s);
+    launch_pad_real(op, S->x.p, 0, S->L, s);
+    fft_forward_r2c(op, s);
+    launch_degrid_plain(op, 0, S->L, S->gold.p, s, true);
     S->precond = op->precond;
     if (S->precond) {
       if (S->projw.n < (size_t)std::max<int64_t>(op->Mtot, 1)) S->projw.alloc(std::max<int64_t>(op->Mtot, 1));
@@ -603,7 +604,7 @@ fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
       if (S->algo == FHS_ALGO_SARA) {
         // sara.m:420-428: proj starts as the projection of G A x0 from zero.
         // With v2 = 0 and gold = G A x0 the dual pass 1 gives d = G A x0 - y.
-        launch_degrid_dual_precond(op, 0, S->L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s);
+        launch_degrid_dual_precond(op, 0, S->L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s, true);
         launch_block_reduce_precond(op, 0, S->L, s);
         launch_fb_iterations(op, 0, S->L, S->projw.p, S->y.p, S->fb_max, S->fb_min, S->fb_stop, s);
       }
