@@ -10,6 +10,7 @@
 // an FP64 Jacobi eigensolve per facet gives V and s_i = sqrt(lambda_i), and
 // the rank-L update is one streaming pass over Z.
 #include "nuclear.cuh"
+#include "tf32.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -88,6 +89,79 @@ __global__ void __launch_bounds__(256) gram_kernel(const NucFacet* __restrict__ 
   for (int e = 0; e < E; ++e) {
     const int ent = threadIdx.x + 256 * e;
     if (ent < lg * lg) out[ent] = acc[e];
+  }
+}
+
+// Gram of up to 16 channels on the tensor cores.  A stage of kGStage pixels
+// of Z is staged channel-major (pitch kGPitch = 4 mod 32: the fragment reads
+// of a warp hit 32 distinct banks); warp w contracts pixels [32 w, 32 w + 32)
+// of the stage: with A = Z^T (16 channels x 8 pixels) the B fragments of the
+// two 8-channel column blocks are A's own elements, so one k-step is four
+// shared loads, one split and 2 x 3 MMAs.  Each stage's products start from
+// zero in the tensor core and are added to the running FP32 sums, so the
+// in-core accumulation never spans more than 32 pixels.
+constexpr int kGStage = 256;
+constexpr int kGPitch = kGStage + 4;
+
+__global__ void __launch_bounds__(256) gram_mma_kernel(const NucFacet* __restrict__ facets, int Q, int lg, int Ny,
+                                                       int64_t npix, const float* __restrict__ xhat,
+                                                       const float* __restrict__ v0, const float* __restrict__ wy,
+                                                       const float* __restrict__ wx, int64_t v0_group,
+                                                       int max_chunks, float* __restrict__ part) {
+  __shared__ float Zs[16 * kGPitch];
+  __shared__ float red[8][256];
+  const int chunk = blockIdx.x, q = blockIdx.y, g = blockIdx.z;
+  const NucFacet f = facets[q];
+  if (chunk >= f.nchunks) return;
+  const int64_t P = (int64_t)(f.y1 - f.y0) * (f.x1 - f.x0);
+  const int64_t c0 = (int64_t)chunk * kNucChunk, c1 = min(P, c0 + kNucChunk);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gr = lane >> 2, t = lane & 3;
+  float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  for (int64_t base = c0; base < c1; base += kGStage) {
+    {
+      const int64_t p = base + threadIdx.x;
+      float z[16];
+      if (p < c1) {
+        load_z_row<16>(f, g, lg, Ny, npix, p, xhat, v0, wy, wx, v0_group, P, z);
+      } else {
+#pragma unroll
+        for (int l = 0; l < 16; ++l) z[l] = 0.f;
+      }
+#pragma unroll
+      for (int l = 0; l < 16; ++l) Zs[l * kGPitch + threadIdx.x] = l < lg ? z[l] : 0.f;
+    }
+    __syncthreads();
+    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      const int k0 = warp * 32 + ks * 8;
+      const float a0 = Zs[gr * kGPitch + k0 + t], a1 = Zs[(gr + 8) * kGPitch + k0 + t];
+      const float a2 = Zs[gr * kGPitch + k0 + t + 4], a3 = Zs[(gr + 8) * kGPitch + k0 + t + 4];
+      const FragA3 A = frag_a3(a0, a1, a2, a3);
+      mma3xtf32(d[0], A, frag_b3(a0, a2));  // channels 0-7
+      mma3xtf32(d[1], A, frag_b3(a1, a3));  // channels 8-15
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[nt][k] += d[nt][k];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt) {
+    red[warp][gr * 16 + 8 * nt + 2 * t] = acc[nt][0];
+    red[warp][gr * 16 + 8 * nt + 2 * t + 1] = acc[nt][1];
+    red[warp][(gr + 8) * 16 + 8 * nt + 2 * t] = acc[nt][2];
+    red[warp][(gr + 8) * 16 + 8 * nt + 2 * t + 1] = acc[nt][3];
+  }
+  __syncthreads();
+  const int i = threadIdx.x >> 4, j = threadIdx.x & 15;
+  if (i < lg && j < lg) {
+    float v = 0.f;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) v += red[w][threadIdx.x];
+    part[(((int64_t)g * Q + q) * max_chunks + chunk) * lg * lg + i * lg + j] = v;
   }
 }
 
@@ -382,8 +456,12 @@ void nuc_plan_init(NucPlan& p, int Ny, int Nx, int Qy, int Qx, const std::vector
 void nuc_gram(const NucPlan& p, const float* xhat, const float* v0, cudaStream_t s) {
   const int64_t npix = (int64_t)p.Ny * p.Nx;
   dim3 grid(p.max_chunks, p.Q, p.n_groups);
-  FHS_NUC_DISPATCH(gram_kernel, grid, p.d_facets.p, p.Q, p.lg, p.Ny, npix, xhat, v0, p.wy.p, p.wx.p, p.v0_group,
-                   p.max_chunks, p.gram_part.p);
+  if (p.lg <= 16)  // tensor cores (3xTF32)
+    gram_mma_kernel<<<grid, 256, 0, s>>>(p.d_facets.p, p.Q, p.lg, p.Ny, npix, xhat, v0, p.wy.p, p.wx.p, p.v0_group,
+                                         p.max_chunks, p.gram_part.p);
+  else
+    FHS_NUC_DISPATCH(gram_kernel, grid, p.d_facets.p, p.Q, p.lg, p.Ny, npix, xhat, v0, p.wy.p, p.wx.p, p.v0_group,
+                     p.max_chunks, p.gram_part.p);
   count_launch();
   FHS_LAUNCH_CHECK();
   gram_reduce_kernel<<<dim3(p.Q, p.n_groups), 256, 0, s>>>(p.d_facets.p, p.Q, p.lg, p.max_chunks, p.gram_part.p,
