@@ -616,6 +616,7 @@ MeasOp::~MeasOp() {
   if (plan_all) cufftDestroy(plan_all);
   if (plan_one) cufftDestroy(plan_one);
   if (plan_r2c) cufftDestroy(plan_r2c);
+  if (plan_c2r) cufftDestroy(plan_c2r);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -924,10 +925,40 @@ void measop_enable_r2c(MeasOp* op) {
   cudaStream_t s = op->stream;
   op->padr.alloc((size_t)op->L * op->No());
   op->padr.zero(s);
+  op->imgr.alloc((size_t)op->L * op->No());
   int n[2] = {op->Kx, op->Ky};
   FHS_CUFFT(cufftPlanMany(&op->plan_r2c, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, op->L));
   FHS_CUFFT(cufftSetStream(op->plan_r2c, s));
+  FHS_CUFFT(cufftPlanMany(&op->plan_c2r, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, op->L));
+  FHS_CUFFT(cufftSetStream(op->plan_c2r, s));
   FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+// H(k) = (B(k) + conj(B(-k))) / 2 on the half plane k0 <= Ky/2: the
+// Hermitian part of the gridded spectrum, whose complex-to-real inverse FFT
+// is Re(IFFT(B)), the only part the adjoint keeps.
+__global__ void hermitian_half_kernel(const float2* __restrict__ B, float2* __restrict__ H, int Ky, int Kx) {
+  const int Kh = Ky / 2 + 1;
+  const int plane = blockIdx.z;
+  const int k1 = blockIdx.y;
+  const int m1 = k1 == 0 ? 0 : Kx - k1;
+  const float2* b = B + (size_t)plane * Kx * Ky;
+  float2* h = H + (size_t)plane * Kx * Kh;
+  for (int k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < Kh; k0 += gridDim.x * blockDim.x) {
+    const float2 u = b[(size_t)k1 * Ky + k0];
+    const float2 v = b[(size_t)m1 * Ky + (k0 == 0 ? 0 : Ky - k0)];
+    h[(size_t)k1 * Kh + k0] = make_float2(0.5f * (u.x + v.x), 0.5f * (u.y - v.y));
+  }
+}
+
+void fft_inverse_c2r(const MeasOp* op, cudaStream_t s) {
+  FHS_CHECK(op->plan_c2r, FHS_ERR_STATE, "real-to-complex path not enabled");
+  const int Kh = op->Ky / 2 + 1;
+  dim3 grid(ceil_div(Kh, 256), op->Kx, op->L);
+  hermitian_half_kernel<<<grid, 256, 0, s>>>(op->gridB.p, op->gridA.p, op->Ky, op->Kx);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  FHS_CUFFT(cufftExecC2R(op->plan_c2r, (cufftComplex*)op->gridA.p, op->imgr.p));
 }
 
 void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s) {

@@ -95,6 +95,10 @@ struct MeasOp {
   // padded real image and its half spectrum (in gridA, [L][Kx][Ky/2 + 1])
   DevBuf<float> padr;
   cufftHandle plan_r2c = 0;
+  // and the complex-to-real adjoint: Hermitian half of gridB (in gridA), its
+  // real inverse FFT [L][Kx][Ky]
+  DevBuf<float> imgr;
+  cufftHandle plan_c2r = 0;
 
   // scratch for API-level calls
   DevBuf<float2> vis_a, vis_b;
@@ -155,6 +159,8 @@ void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStre
 void measop_enable_r2c(MeasOp* op);
 void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s);
 void fft_forward_r2c(const MeasOp* op, cudaStream_t s);
+// imgr <- Re(IFFT(gridB)) of all L planes (Hermitian half into gridA, then C2R)
+void fft_inverse_c2r(const MeasOp* op, cudaStream_t s);
 // gridB <- G^H v (v sorted, channels [c0, c0+nc)); non-empty tiles only
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
 // out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1

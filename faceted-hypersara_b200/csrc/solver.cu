@@ -93,21 +93,21 @@ struct AssembleArgs {
 };
 
 __global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, float* __restrict__ g,
-                                                       const float2* __restrict__ gridA, const float* __restrict__ g1,
+                                                       const float* __restrict__ img, const float* __restrict__ g1,
                                                        const float* __restrict__ v0, const float* __restrict__ sigma22,
                                                        const float* __restrict__ sy, const float* __restrict__ sx) {
   const int plane = blockIdx.y;
   const int grp = plane / a.lg, lc = plane - grp * a.lg;
   const int64_t N = (int64_t)a.Ny * a.Nx;
   const float s22 = sigma22[plane];
-  const float2* gp = gridA + (size_t)plane * a.Ky * a.Kx;
+  const float* gp = img + (size_t)plane * a.Ky * a.Kx;  // Re(IFFT(gridB)), [Kx][Ky]
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
     const int ix = (int)(p / a.Ny), iy = (int)(p - (int64_t)ix * a.Ny);
     int ky = iy - a.Ny / 2;
     ky += ky < 0 ? a.Ky : 0;
     int kx = ix - a.Nx / 2;
     kx += kx < 0 ? a.Kx : 0;
-    float val = s22 * sy[iy] * sx[ix] * gp[(size_t)kx * a.Ky + ky].x + g1[(size_t)plane * N + p];
+    float val = s22 * sy[iy] * sx[ix] * gp[(size_t)kx * a.Ky + ky] + g1[(size_t)plane * N + p];
     if (a.nuclear) {
       float acc = 0.f;
       for (int i = 0; i < 2; ++i) {
@@ -264,7 +264,7 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
     launch_grid_dual(op, 0, L, S->v2.p, s);
     mark();
   }
-  fft_inverse(op, 0, L, s);
+  fft_inverse_c2r(op, s);
   mark();
   FHS_CUDA(cudaMemsetAsync(S->l21_acc.p, 0, S->G * sizeof(double), s));
   if (sara_fused_supported(S->lg)) {
@@ -299,7 +299,7 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   a.cover_y = S->nuclear ? S->np.cover_y.p : nullptr;
   a.cover_x = S->nuclear ? S->np.cover_x.p : nullptr;
   a.v0_group = S->nuclear ? S->np.v0_group : 0;
-  assemble_kernel<<<dim3(nblk(S->N), L), 256, 0, s>>>(a, S->g.p, op->gridA.p, S->g1.p, S->v0.p, S->sigma22.p,
+  assemble_kernel<<<dim3(nblk(S->N), L), 256, 0, s>>>(a, S->g.p, op->imgr.p, S->g1.p, S->v0.p, S->sigma22.p,
                                                      op->sy.p, op->sx.p);
   count_launch();
   FHS_LAUNCH_CHECK();
