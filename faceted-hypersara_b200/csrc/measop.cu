@@ -81,7 +81,7 @@ __device__ __forceinline__ int wrap(int k, int K) {
 // HALF: the grid is the half spectrum of a real-to-complex FFT,
 // [Kx][Ky/2 + 1] per channel; G(k0, k1) for k0 > Ky/2 is conj(G(-k0, -k1)).
 template <int J, int MODE, int NB, bool HALF>
-__global__ void __launch_bounds__(256) degrid_kernel(OpView op, const float2* __restrict__ grid,
+__global__ void __launch_bounds__(256, 3) degrid_kernel(OpView op, const float2* __restrict__ grid,
                                                      const WorkItem* __restrict__ items,
                                                      const int* __restrict__ order, int item0,
                                                      float2* __restrict__ out, const float2* __restrict__ v2,
