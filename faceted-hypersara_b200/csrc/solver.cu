@@ -759,6 +759,113 @@ fhs_status fhs_solver_ellipse_iterations(fhs_solver* s_, int* counts) {
   });
 }
 
+}  // extern "C"
+
+namespace fhs {
+namespace {
+
+// Number of doubles of one state field in the host layout (0: not present).
+int64_t field_size(const Solver* S, int field) {
+  const MeasOp* op = S->op;
+  const int64_t LN = (int64_t)S->L * S->N;
+  switch (field) {
+    case FHS_FIELD_X:
+    case FHS_FIELD_G:
+      return LN;
+    case FHS_FIELD_V0:
+      return S->nuclear ? (int64_t)S->G * S->np.v0_group : 0;
+    case FHS_FIELD_V1:
+      return (int64_t)S->L * S->sp.s;
+    case FHS_FIELD_V2:
+      return 2 * op->Mtot;
+    case FHS_FIELD_PROJ:
+      return S->precond ? 2 * op->Mtot : 0;
+    case FHS_FIELD_WEIGHTS0:
+      return S->nuclear ? (int64_t)S->G * S->np.Q * S->lg : 0;
+    case FHS_FIELD_WEIGHTS1:
+      return (int64_t)S->G * S->sp.s;
+    default:
+      return -1;
+  }
+}
+
+float* float_field(Solver* S, int field) {
+  switch (field) {
+    case FHS_FIELD_X: return S->x.p;
+    case FHS_FIELD_G: return S->g.p;
+    case FHS_FIELD_V0: return S->v0.p;
+    case FHS_FIELD_V1: return S->v1.p;
+    case FHS_FIELD_WEIGHTS1: return S->w1.p;
+    default: return nullptr;
+  }
+}
+
+void state_io(Solver* S, int field, double* out, const double* in) {
+  FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+  const int64_t n = field_size(S, field);
+  FHS_CHECK(n >= 0, FHS_ERR_INVALID_ARG, "unknown state field");
+  if (n == 0) return;
+  FHS_CHECK(out || in, FHS_ERR_INVALID_ARG, "null buffer");
+  MeasOp* op = S->op;
+  DeviceGuard dg(op->device);
+  cudaStream_t s = op->stream;
+  if (op->stage.n < (size_t)n) op->stage.alloc(n);
+  double* st = op->stage.p;
+  if (in) FHS_CUDA(cudaMemcpyAsync(st, in, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  switch (field) {
+    case FHS_FIELD_V2:
+      if (in)
+        launch_vis_gather(st, S->v2.p, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
+      else
+        launch_vis_scatter(S->v2.p, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
+      break;
+    case FHS_FIELD_PROJ:
+      if (in)
+        launch_w_from_proj(op, st, S->y.p, S->projw.p, s);
+      else
+        launch_proj_from_w(op, S->projw.p, S->y.p, st, s);
+      break;
+    case FHS_FIELD_WEIGHTS0:
+      if (in)
+        FHS_CUDA(cudaMemcpyAsync(S->w0.p, st, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      else
+        FHS_CUDA(cudaMemcpyAsync(st, S->w0.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      break;
+    default:
+      if (in)
+        launch_d2f(st, float_field(S, field), n, s);
+      else
+        launch_f2d(float_field(S, field), st, n, s);
+  }
+  if (out) FHS_CUDA(cudaMemcpyAsync(out, st, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace fhs
+
+extern "C" {
+
+int64_t fhs_solver_field_size(const fhs_solver* s_, int field) {
+  const Solver* S = reinterpret_cast<const Solver*>(s_);
+  if (!S) return -1;
+  return field_size(S, field);
+}
+
+fhs_status fhs_solver_get_field(fhs_solver* s_, int field, double* out) {
+  return guarded_solver([&] {
+    FHS_CHECK(out != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    state_io(sv(s_), field, out, nullptr);
+  });
+}
+
+fhs_status fhs_solver_set_field(fhs_solver* s_, int field, const double* in) {
+  return guarded_solver([&] {
+    FHS_CHECK(in != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    state_io(sv(s_), field, nullptr, in);
+  });
+}
+
 int fhs_solver_stage_count(void) { return kStages; }
 
 const char* fhs_solver_stage_name(int i) { return (i >= 0 && i < kStages) ? kStageNames[i] : ""; }

@@ -5,4 +5,5 @@ behind the C ABI of ``include/fhs_b200.h``).
 """
 from ._lib import FhsError, lib  # noqa: F401
 from .api import *  # noqa: F401,F403
-from . import heuristics, synth  # noqa: F401
+from . import heuristics, io, synth  # noqa: F401
+from .io import fitsread, fitswrite, load_checkpoint, save_checkpoint  # noqa: F401

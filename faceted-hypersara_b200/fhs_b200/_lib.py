@@ -108,11 +108,17 @@ SIGNATURES = {
     "fhs_solver_get_x": (C.c_int, [_vp, _dp]),
     "fhs_solver_update_weights": (C.c_int, [_vp]),
     "fhs_solver_ellipse_iterations": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "fhs_solver_field_size": (C.c_int64, [_vp, C.c_int]),
+    "fhs_solver_get_field": (C.c_int, [_vp, C.c_int, _dp]),
+    "fhs_solver_set_field": (C.c_int, [_vp, C.c_int, _dp]),
     "fhs_solver_stage_count": (C.c_int, []),
     "fhs_solver_stage_name": (C.c_char_p, [C.c_int]),
     "fhs_solver_time_iterations": (C.c_int, [_vp, C.c_int, _dp]),
     "fhs_solver_profile_stages": (C.c_int, [_vp, C.c_int, _dp]),
 }
+
+# fhs_field (include/fhs_b200.h)
+FIELDS = {"xsol": 0, "g": 1, "v0": 2, "v1": 3, "v2": 4, "proj": 5, "weights0": 6, "weights1": 7}
 
 _lib = None
 

@@ -466,6 +466,53 @@ class Solver:
     def update_weights(self):
         check(lib().fhs_solver_update_weights(self._h))
 
+    def get_state(self):
+        """The solver state the reference checkpoints (facetHyperSARA.m:1071-1107):
+        dict xsol/g [Ny, Nx, L], v0 (flat, per group and facet [P_q, lg]),
+        v1 [s, L], v2/proj (nested [l][b] complex), weights0 [lg, Q, groups],
+        weights1 [s, groups]; absent fields are omitted."""
+        op = self.op
+        out = {}
+        for name, f in LB.FIELDS.items():
+            n = int(lib().fhs_solver_field_size(self._h, f))
+            if n <= 0:
+                continue
+            a = np.empty(n)
+            check(lib().fhs_solver_get_field(self._h, f, dptr(a)))
+            if name in ("xsol", "g"):
+                a = a.reshape(op.Ny, op.Nx, op.L, order="F")
+            elif name == "v1":
+                a = a.reshape(-1, op.L, order="F")
+            elif name == "weights1":
+                a = a.reshape(-1, self.G, order="F")
+            elif name == "weights0":
+                a = a.reshape(-1, self.Q, self.G, order="F")
+            elif name in ("v2", "proj"):
+                c, res, pos = a.view(np.complex128), [], 0
+                for l in range(op.L):
+                    res.append(op.split(l, c[pos:pos + op.n_vis[l]].copy()))
+                    pos += op.n_vis[l]
+                a = res
+            out[name] = a
+        return out
+
+    def set_state(self, state):
+        """Restores fields of get_state (after init); unknown keys are ignored."""
+        for name, f in LB.FIELDS.items():
+            if name not in state:
+                continue
+            n = int(lib().fhs_solver_field_size(self._h, f))
+            if n <= 0:
+                continue
+            v = state[name]
+            if name in ("v2", "proj"):
+                a = _cplx_in(np.concatenate([self.op.flatten(b) for b in v]))
+            else:
+                a = _f64(np.asarray(v, dtype=np.float64).reshape(-1, order="F"))
+            if a.size != n:
+                raise ValueError(f"state field {name}: expected {n} values, got {a.size}")
+            check(lib().fhs_solver_set_field(self._h, f, dptr(a)))
+
     def ellipse_iterations(self):
         """FB iterations of the ellipsoid projection per block in the last
         iteration (nested [l][b]; zeros without a preconditioner)."""

@@ -269,6 +269,37 @@ FHS_API fhs_status fhs_solver_get_x(fhs_solver* s, double* x);
  * The reference's solver_proj_elipse_fb returns the same count as its second
  * output (src/sara/sara.m:561). */
 FHS_API fhs_status fhs_solver_ellipse_iterations(fhs_solver* s, int* counts);
+
+/* Solver state for checkpoints and warm restarts: the arrays the reference
+ * saves in its checkpoint files (src/fhs/facetHyperSARA.m:1071-1107: xsol, g,
+ * v0, v1, v2, proj, weights0, weights1) and reads back on a warm start
+ * (src/fhs/fhs_initialize_dual_and_weights.m, src/sara/sara.m:394-400).
+ * Host layouts (doubles, column-major as MATLAB):
+ *   X, G       [Ny, Nx, L]
+ *   V0         per group, per facet [P_q, lg] (group-major, facets in
+ *              column-major facet order), the nuclear-norm duals
+ *   V1         [s, L], s = fhs_sara_n_coefs (SARA coefficient layout of
+ *              fhs_sara_analysis), the l21 duals
+ *   V2, PROJ   all channels' visibilities, interleaved complex, in the
+ *              channels' visibility order (PROJ only with a preconditioner)
+ *   WEIGHTS0   [lg, Q, n_groups] (group-major: g * Q * lg + q * lg + l)
+ *   WEIGHTS1   [s, n_groups]
+ * Set fields after fhs_solver_init (which derives the data-term cache from x):
+ * the next iteration continues from the restored state. */
+typedef enum fhs_field {
+  FHS_FIELD_X = 0,
+  FHS_FIELD_G = 1,
+  FHS_FIELD_V0 = 2,
+  FHS_FIELD_V1 = 3,
+  FHS_FIELD_V2 = 4,
+  FHS_FIELD_PROJ = 5,
+  FHS_FIELD_WEIGHTS0 = 6,
+  FHS_FIELD_WEIGHTS1 = 7
+} fhs_field;
+/* doubles of a field in the host layout (0: not present, -1: unknown field) */
+FHS_API int64_t fhs_solver_field_size(const fhs_solver* s, int field);
+FHS_API fhs_status fhs_solver_get_field(fhs_solver* s, int field, double* out);
+FHS_API fhs_status fhs_solver_set_field(fhs_solver* s, int field, const double* in);
 /* Recompute reweighting weights from the current x (fhs_update_weights.m). */
 FHS_API fhs_status fhs_solver_update_weights(fhs_solver* s);
 
