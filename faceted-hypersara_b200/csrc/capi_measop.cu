@@ -196,6 +196,58 @@ int64_t fhs_measop_n_vis(const fhs_measop* op, int channel) {
   return m->ch[channel].M;
 }
 
+fhs_status fhs_measop_create_dr(fhs_measop* vis, fhs_measop** out) {
+  return guarded([&] {
+    FHS_CHECK(out != nullptr, FHS_ERR_INVALID_ARG, "null output handle");
+    *out = nullptr;
+    MeasOp* v = committed(vis);
+    FHS_CHECK(!v->precond, FHS_ERR_UNSUPPORTED, "no dimensionality reduction of a preconditioned operator");
+    *out = reinterpret_cast<fhs_measop*>(measop_create_dr(v));
+  });
+}
+
+int fhs_measop_is_dr(const fhs_measop* op) {
+  const MeasOp* m = reinterpret_cast<const MeasOp*>(op);
+  return m ? (m->dr ? 1 : 0) : -1;
+}
+
+static MeasOp* dr_channel(fhs_measop* op_, int channel) {
+  MeasOp* op = committed(op_);
+  FHS_CHECK(op->dr, FHS_ERR_STATE, "not a dimensionality-reduced operator");
+  FHS_CHECK(channel >= 0 && channel < op->L, FHS_ERR_INVALID_ARG, "bad channel index");
+  return op;
+}
+
+fhs_status fhs_measop_dr_cells(fhs_measop* op_, int channel, int64_t* cells) {
+  return guarded([&] {
+    MeasOp* op = dr_channel(op_, channel);
+    const int64_t n = op->h_M[channel];
+    FHS_CHECK(n == 0 || cells, FHS_ERR_INVALID_ARG, "null buffer");
+    if (n == 0) return;
+    DeviceGuard g(op->device);
+    std::vector<int32_t> h(n);
+    op->dr_cell.download_at(h.data(), op->h_voff[channel], n, op->stream);
+    FHS_CUDA(cudaStreamSynchronize(op->stream));
+    for (int64_t i = 0; i < n; ++i) cells[i] = h[i];
+  });
+}
+
+fhs_status fhs_measop_dr_lambda(fhs_measop* op_, int channel, double* lambda) {
+  return guarded([&] {
+    MeasOp* op = dr_channel(op_, channel);
+    const int64_t n = op->h_M[channel];
+    FHS_CHECK(n == 0 || lambda, FHS_ERR_INVALID_ARG, "null buffer");
+    if (n == 0) return;
+    DeviceGuard g(op->device);
+    std::vector<int32_t> cell(n);
+    op->dr_cell.download_at(cell.data(), op->h_voff[channel], n, op->stream);
+    std::vector<float2> w((size_t)op->No());
+    op->dr_omega.download_at(w.data(), (size_t)channel * op->No(), op->No(), op->stream);
+    FHS_CUDA(cudaStreamSynchronize(op->stream));
+    for (int64_t i = 0; i < n; ++i) lambda[i] = std::hypot((double)w[cell[i]].x, (double)w[cell[i]].y);
+  });
+}
+
 int64_t fhs_measop_grid_size(const fhs_measop* op) {
   const MeasOp* m = reinterpret_cast<const MeasOp*>(op);
   return m ? m->No() : -1;

@@ -79,6 +79,10 @@ struct DevBuf {
     FHS_CHECK(count <= n, FHS_ERR_INVALID_ARG, "download larger than buffer");
     if (count) FHS_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
   }
+  void download_at(T* h, size_t first, size_t count, cudaStream_t s) const {
+    FHS_CHECK(first + count <= n, FHS_ERR_INVALID_ARG, "download beyond buffer");
+    if (count) FHS_CUDA(cudaMemcpyAsync(h, p + first, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
 };
 
 // Makes a device current for the lifetime of the guard.

@@ -300,6 +300,8 @@ void advance(const MeasOp* op, int i0, int n, double2* w, const float2* y, cudaS
 
 void measop_set_preconditioner(MeasOp* op, int c, const double* pu) {
   FHS_CHECK(op->committed, FHS_ERR_STATE, "commit the operator before setting a preconditioner");
+  // util_load_data_gen_dr_measurement_operator.m:118: no preconditioning with DR
+  FHS_CHECK(!op->dr, FHS_ERR_UNSUPPORTED, "no preconditioner on a dimensionality-reduced operator");
   FHS_CHECK(c >= 0 && c < op->L, FHS_ERR_INVALID_ARG, "bad channel index");
   const int M = op->h_M[c];
   FHS_CHECK(M == 0 || pu != nullptr, FHS_ERR_INVALID_ARG, "null preconditioner");

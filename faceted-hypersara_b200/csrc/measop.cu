@@ -26,6 +26,7 @@
 // or in the 8-cell ring below it, then writes the tile once: no atomics of
 // any kind, no grid zeroing.
 #include "measop.cuh"
+#include "cplx.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -39,38 +40,6 @@ unsigned long long g_launches = 0;
 namespace {
 
 constexpr int kSmemPitch = kTileCells + kBinCells;  // 72 (>= 64 + J - 1)
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // conj(a) * b
-  return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
-}
-__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {  // a*b + c
-  return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
-}
-
-// Tap coefficients h_j(f) of one axis by Horner evaluation of degree-8
-// polynomials in f - 1/2 (FP32, < 1e-7 relative to the FP64 construction).
-template <int J>
-__device__ __forceinline__ void taps(const float (&P)[kMaxTaps][2][kPolyDegree + 1], float f, float2 (&h)[J]) {
-  const float s = f - 0.5f;
-#pragma unroll
-  for (int j = 0; j < J; ++j) {
-    float re = P[j][0][kPolyDegree], im = P[j][1][kPolyDegree];
-#pragma unroll
-    for (int k = kPolyDegree - 1; k >= 0; --k) {
-      re = fmaf(re, s, P[j][0][k]);
-      im = fmaf(im, s, P[j][1][k]);
-    }
-    h[j] = make_float2(re, im);
-  }
-}
-
-__device__ __forceinline__ int wrap(int k, int K) {
-  k %= K;
-  return k < 0 ? k + K : k;
-}
 
 // ---------------------------------------------------------------- degrid
 // MODE 0: out = G Fx.  MODE 1: l2-ball dual, pass 1.  MODE 2: ellipsoid dual,
@@ -856,20 +825,26 @@ void measop_commit(MeasOp* op) {
   };
   upload_table(op->ay, op->tab_y, op->sy);
   upload_table(op->ax, op->tab_x, op->sx);
-  op->geom.alloc(std::max<int64_t>(op->Mtot, 1));
+  // a DR operator (measop_create_dr) has no visibility geometry: its data
+  // entries are grid cells, in order (perm = identity)
+  if (!op->dr) {
+    op->geom.alloc(std::max<int64_t>(op->Mtot, 1));
+    op->sb_off.alloc((size_t)L * (op->nkeys + 1));
+  }
   op->zbuf.alloc(std::max<int64_t>(op->Mtot, 1));
   op->perm.alloc(std::max<int64_t>(op->Mtot, 1));
-  op->sb_off.alloc((size_t)L * (op->nkeys + 1));
   for (int c = 0; c < L; ++c) {
     const ChannelHost& h = op->ch[c];
     if (h.M) {
-      FHS_CUDA(cudaMemcpyAsync(op->geom.p + op->h_voff[c], h.geom.data(), h.M * sizeof(float4),
-                               cudaMemcpyHostToDevice, s));
+      if (!op->dr)
+        FHS_CUDA(cudaMemcpyAsync(op->geom.p + op->h_voff[c], h.geom.data(), h.M * sizeof(float4),
+                                 cudaMemcpyHostToDevice, s));
       FHS_CUDA(cudaMemcpyAsync(op->perm.p + op->h_voff[c], h.perm.data(), h.M * sizeof(int32_t),
                                cudaMemcpyHostToDevice, s));
     }
-    FHS_CUDA(cudaMemcpyAsync(op->sb_off.p + (size_t)c * (op->nkeys + 1), h.sb_off.data(),
-                             (op->nkeys + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    if (!op->dr)
+      FHS_CUDA(cudaMemcpyAsync(op->sb_off.p + (size_t)c * (op->nkeys + 1), h.sb_off.data(),
+                               (op->nkeys + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   }
   op->ch_voff.alloc(L);
   op->ch_voff.upload(op->h_voff.data(), L, s);
@@ -885,7 +860,10 @@ void measop_commit(MeasOp* op) {
   op->gridA.alloc(gsz);
   op->gridB.alloc(gsz);
   op->gridB.zero(s);
-  build_work_lists(op, s);
+  if (op->dr)
+    measop_dr_lists(op, s);
+  else
+    build_work_lists(op, s);
   op->blk_stats.alloc((size_t)std::max(op->nblk_tot, 1) * 2);
   op->blk_scale.alloc((size_t)L * kMaxBlocksPerChannel);
   op->blk_scale.zero(s);
@@ -1011,6 +989,7 @@ PrecondView MeasOp::precond_view(const double2* w) const {
 }
 
 void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStream_t s, bool half) {
+  if (op->dr) return launch_dr_apply(op, 0, c0, nc, nullptr, out, nullptr, nullptr, nullptr, s, half);
   const int i0 = op->h_dg_off[c0], n = op->h_dg_off[c0 + nc] - i0;
   if (n == 0) return;
   if (half)
@@ -1024,6 +1003,7 @@ void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStre
 }
 
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s) {
+  if (op->dr) return launch_dr_apply(op, 3, c0, nc, v, nullptr, nullptr, nullptr, nullptr, s, false);
   launch_grid_kernel<7, 0>(op, c0, nc, v, nullptr, nullptr, nullptr, PrecondView{}, s);
 }
 
@@ -1072,6 +1052,7 @@ static void degrid_dual_nb(const MeasOp* op, int c0, int nc, const float2* v2, f
 
 void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
                         cudaStream_t s, bool half) {
+  if (op->dr) return launch_dr_apply(op, 1, c0, nc, nullptr, nullptr, v2, gold, y, s, half);
   degrid_dual_nb<1>(op, c0, nc, v2, gold, y, PrecondView{}, s, half);
 }
 
@@ -1097,6 +1078,7 @@ void launch_block_reduce_precond(const MeasOp* op, int c0, int nc, cudaStream_t 
 }
 
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s) {
+  if (op->dr) return launch_dr_apply(op, 2, c0, nc, nullptr, nullptr, v2, nullptr, nullptr, s, false);
   launch_grid_kernel<7, 1>(op, c0, nc, nullptr, v2, op->blk_scale.p, op->zbuf.p, PrecondView{}, s);
 }
 

@@ -132,6 +132,17 @@ struct MeasOp {
   DevBuf<int> fb_off;
   DevBuf<double> fb_part;                 // [fb items][kMaxBlocksPerChannel][3]
 
+  // dimensionality reduction (visibility gridding, measop_create_dr): the
+  // data space of channel c is its active grid cells W_c (diag(G^H G) > 0) in
+  // column-major order; the operator is Lambda H on W_c with H = G^H G kept as
+  // a half stencil T (diagonal halved, H = T + T^H) over the whole grid.
+  bool dr = false;
+  DevBuf<float2> dr_T;      // [L][kDrHalf][Kx][Ky]
+  DevBuf<float2> dr_omega;  // [L][Kx][Ky] Lambda conj(rho): Lambda = diag(H)^-1/2 on W_c, 0 elsewhere
+  DevBuf<int32_t> dr_map;   // [L][Kx][Ky] data index (channel-relative) of each cell, -1 off W_c
+  DevBuf<int32_t> dr_cell;  // [Mtot] grid cell of each data entry
+  int dr_tiles = 0;         // apply tiles per channel
+
   int64_t No() const { return (int64_t)Ky * Kx; }
   int64_t Npix() const { return (int64_t)Ny * Nx; }
   int ntiles() const { return nT0 * nT1; }
@@ -172,6 +183,22 @@ void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* go
 void launch_block_reduce(const MeasOp* op, int c0, int nc, cudaStream_t s);
 // fused dual update, pass 2: v2 <- zbuf*scale, gridB <- G^H v2
 void launch_grid_dual(const MeasOp* op, int c0, int nc, float2* v2, cudaStream_t s);
+
+// ---- dimensionality reduction (visibility gridding, see dr.cu) ----------
+// 13 x 13 coupling stencil of two 7-tap supports; its half: the diagonal and
+// the 84 offsets (d0, d1) with d1 < 0 or (d1 == 0 and d0 < 0)
+constexpr int kDrReach = 6;
+constexpr int kDrHalf = ((2 * kDrReach + 1) * (2 * kDrReach + 1) + 1) / 2;  // 85
+// builds the DR operator of a committed visibility operator (one block per
+// channel); the result is committed
+MeasOp* measop_create_dr(const MeasOp* vis);
+// per-(channel, apply tile) partial-sum slots of the DR dual (measop_commit)
+void measop_dr_lists(MeasOp* op, cudaStream_t s);
+// MODE 0: out = Lambda (H Fx)(W) (gridA, half: R2C half spectrum).  MODE 1:
+// l2-ball dual pass 1.  MODE 2: dual pass 2 (v2 = z scale, gridB = H Lambda v2).
+// MODE 3: gridB = H (Lambda v).  (Centring phase folded in, see dr.cu.)
+void launch_dr_apply(const MeasOp* op, int mode, int c0, int nc, const float2* vin, float2* out, float2* v2,
+                     float2* gold, const float2* y, cudaStream_t s, bool half);
 
 // ---- preconditioned dual (ellipsoid projection, see ellipse.cu) ---------
 // pU of one channel in its original visibility order (requires a committed op)

@@ -396,6 +396,7 @@ fhs_status fhs_solver_create(fhs_measop* op_, const fhs_solver_config* cfg, fhs_
     cudaStream_t s = op->stream;
     auto S = std::make_unique<Solver>();
     S->op = op;
+    S->device = op->device;
     S->algo = cfg->algo;
     S->nlevel = cfg->nlevel > 0 ? cfg->nlevel : 4;
     S->L = op->L;
@@ -475,7 +476,7 @@ fhs_status fhs_solver_destroy(fhs_solver* s) {
   return guarded_solver([&] {
     Solver* S = reinterpret_cast<Solver*>(s);
     if (!S) return;
-    DeviceGuard dg(S->op->device);
+    DeviceGuard dg(S->device);
     delete S;
   });
 }

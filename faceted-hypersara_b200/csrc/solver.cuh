@@ -12,6 +12,7 @@ constexpr int kReportRing = 1024;  // iterations kept on the device between host
 
 struct Solver {
   MeasOp* op = nullptr;
+  int device = 0;               // op->device, kept so that destroy never reads op
   int algo = FHS_ALGO_FHS, nlevel = 4, G = 1, lg = 1, L = 1, Ny = 0, Nx = 0;
   int64_t N = 0;
   SaraPlan sp;

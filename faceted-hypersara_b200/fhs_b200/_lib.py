@@ -72,6 +72,10 @@ SIGNATURES = {
     "fhs_measop_set_channel": (C.c_int, [_vp, C.c_int, C.c_int64, _dp, _dp, _dp, C.c_int, _i64p]),
     "fhs_measop_commit": (C.c_int, [_vp]),
     "fhs_measop_n_vis": (C.c_int64, [_vp, C.c_int]),
+    "fhs_measop_create_dr": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "fhs_measop_is_dr": (C.c_int, [_vp]),
+    "fhs_measop_dr_cells": (C.c_int, [_vp, C.c_int, _i64p]),
+    "fhs_measop_dr_lambda": (C.c_int, [_vp, C.c_int, _dp]),
     "fhs_measop_grid_size": (C.c_int64, [_vp]),
     "fhs_scaled_fft": (C.c_int, [_vp, _dp, _dp]),
     "fhs_scaled_fft_adjoint": (C.c_int, [_vp, _dp, _dp]),

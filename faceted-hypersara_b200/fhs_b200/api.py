@@ -81,9 +81,59 @@ class MeasurementOperator:
         self.n_vis = [int(lib().fhs_measop_n_vis(h, l)) for l in range(self.L)]
         self.n_vis_total = int(sum(self.n_vis))
 
+    @classmethod
+    def _from_dr_handle(cls, h, vis):
+        self = cls.__new__(cls)
+        self._h = h
+        self.Ny, self.Nx, self.L = vis.Ny, vis.Nx, vis.L
+        self.Ky, self.Kx, self.No = vis.Ky, vis.Kx, vis.No
+        self.device = vis.device
+        self.n_vis = [int(lib().fhs_measop_n_vis(h, l)) for l in range(self.L)]
+        self.n_vis_total = int(sum(self.n_vis))
+        self.block_sizes = [[n] for n in self.n_vis]
+        self.W, self.Lambda = [], []
+        for l, n in enumerate(self.n_vis):
+            cells = np.empty(n, dtype=np.int64)
+            lam = np.empty(n)
+            check(lib().fhs_measop_dr_cells(h, l, cells.ctypes.data_as(C.POINTER(C.c_int64))))
+            check(lib().fhs_measop_dr_lambda(h, l, dptr(lam)))
+            self.W.append(cells)
+            self.Lambda.append(lam)
+        return self
+
     @property
     def handle(self):
         return self._h
+
+    @property
+    def is_dr(self):
+        return bool(lib().fhs_measop_is_dr(self._h) == 1)
+
+    def dimensionality_reduction(self):
+        """lib/operators/util_load_data_gen_dr_measurement_operator.m:109-228:
+        the visibility-gridding operator of this one (H = G'G over each
+        channel's blocks, W = diag(H) > 0, Lambda = diag(H)^-1/2, one block per
+        channel).  Returns a MeasurementOperator whose data entries of channel
+        l are the active cells ``W[l]`` (0-based column-major grid indices,
+        ascending) with weights ``Lambda[l]``; the operator functions, the
+        dual update and the solvers take it in place of this one."""
+        h = C.c_void_p()
+        check(lib().fhs_measop_create_dr(self._h, C.byref(h)))
+        return MeasurementOperator._from_dr_handle(h, self)
+
+    def reduce_data(self, dr, y):
+        """Lambda .* (G' y)(W) per channel (util_load_data_gen_dr_measurement_
+        operator.m:180, 219): the gridded data of visibilities ``y[l]`` (one
+        array or a list of blocks per channel) for the DR operator ``dr`` made
+        from this operator, as ``[[y_dr_l]]``.  Applied to a noise draw it
+        gives the gridded noise whose norm is the DR l2 bound (:184-201, 226)."""
+        out = []
+        for l in range(self.L):
+            yl = y[l]
+            v = self.flatten(yl) if isinstance(yl, (list, tuple)) else np.asarray(yl, dtype=np.complex128)
+            g = apply_adjoint_operator(v, self, l)
+            out.append([dr.Lambda[l] * g[dr.W[l]]])
+        return out
 
     def close(self):
         if getattr(self, "_h", None):

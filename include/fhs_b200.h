@@ -149,6 +149,34 @@ FHS_API fhs_status fhs_update_dual_data_fidelity_precond(fhs_measop* op, double*
                                                          double* global_norm_res, double* norm_epsilon,
                                                          int* fb_iters);
 
+/* ----------------------------------------------------------------------
+ * Visibility gridding / dimensionality reduction (DR): the operator built by
+ * lib/operators/util_load_data_gen_dr_measurement_operator.m:109-228 and the
+ * flag_visibility_gridding branches of update_dual_data_fidelity.m:85-125,
+ * HS_forward_operator_G.m:41-45, HS_adjoint_operator_G.m:46-49,
+ * compute_residual_images.m:42-80 and util_operator_norm.m
+ * ---------------------------------------------------------------------- */
+/* Builds the DR operator of a committed visibility operator: per channel
+ * H = G'G over all its blocks, W = diag(H) > 0, Lambda = diag(H)^-1/2 on W,
+ * one data block per channel (the reference's "1 single block per channel").
+ * The result is a committed operator of the same image and grid sizes whose
+ * data entries of channel l are the n_vis(l) = |W_l| active grid cells in
+ * column-major order (the order of MATLAB's Fx(W)).  On it the calls above
+ * apply the reference's DR formulas: apply_direct / forward: y =
+ * Lambda .* (H Fx)(W); apply_adjoint / adjoint: g2(W) = H (Lambda .* y);
+ * residual images, operator norm, the l2-ball dual update and the solvers
+ * likewise.  No preconditioner (util_load_data_gen_dr_measurement_operator.m:
+ * 118).  The visibility operator stays valid and independent. */
+FHS_API fhs_status fhs_measop_create_dr(fhs_measop* vis_op, fhs_measop** dr_op);
+/* 1 for an operator made by fhs_measop_create_dr, 0 otherwise, -1 null. */
+FHS_API int fhs_measop_is_dr(const fhs_measop* op);
+/* W{l}: the 0-based column-major grid index of each data entry of channel l
+ * (n_vis(l) values). */
+FHS_API fhs_status fhs_measop_dr_cells(fhs_measop* op, int channel, int64_t* cells);
+/* Lambda{l}: diag(H)^-1/2 of each data entry of channel l (n_vis(l) values,
+ * FP32 precision of the device copy). */
+FHS_API fhs_status fhs_measop_dr_lambda(fhs_measop* op, int channel, double* lambda);
+
 /* ======================================================================
  * Priors (standalone, device selected per call)
  * ====================================================================== */
@@ -247,6 +275,9 @@ typedef struct fhs_run_info {
 
 typedef struct fhs_solver fhs_solver;
 
+/* The solver uses op (grids, FFT plans, data layout) on every call: op must
+ * outlive every call but the destroy, which touches only the solver's own
+ * memory and may come after fhs_measop_destroy. */
 FHS_API fhs_status fhs_solver_create(fhs_measop* op, const fhs_solver_config* cfg, fhs_solver** out);
 FHS_API fhs_status fhs_solver_destroy(fhs_solver* s);
 /* y: visibilities of all channels (whitened, original order); epsilon: one l2

@@ -245,3 +245,59 @@ def test_uniform_weight_preconditioner_counts():
     om_x = np.array([2 * g, 2.3 * g, 1.9 * g, 0.1 * g, 0.0])
     pU = so.uniform_weight_preconditioner(om_y, om_x, Ky, Kx)
     assert np.allclose(pU, [1 / 3, 1 / 3, 1 / 3, 1.0, 1.0])
+
+
+def test_dr_operator_equals_gram_on_active_cells():
+    """util_load_data_gen_dr_measurement_operator.m: the tril / half-diagonal
+    H applied as H u + (u'H)' is G'G on the active cells; Lambda normalises
+    diag(G'G) to 1; the DR matrix form equals the istril formulas."""
+    from oracle import dr
+    data, x, meta = problem.make_problem(16, 24, 1, 700, 3, seed=5, synth=synth)
+    G = data.G[0]
+    H, W, lam = dr.dr_operator(G, data.op.No)
+    Gfull = sum((Gb.conj().T @ Gb) for Gb in G).toarray()
+    assert np.array_equal(W, np.diag(Gfull).real > 0)
+    assert 0 < W.sum() < W.size
+    Hf = (H + H.conj().T).toarray()
+    assert np.allclose(Hf, Gfull[np.ix_(W, W)], rtol=0, atol=1e-12 * np.abs(Gfull).max())
+    assert np.allclose(lam ** 2 * np.diag(Hf).real, 1.0)
+    rng = np.random.default_rng(0)
+    Fx = rng.standard_normal(data.op.No) + 1j * rng.standard_normal(data.op.No)
+    y = dr.dr_forward(H, lam, Fx[W])
+    Gdr = dr.dr_matrix(H, W, lam)
+    assert np.allclose(Gdr @ Fx, y)
+    assert np.allclose(y, lam * (Gfull @ Fx)[W])
+    v = rng.standard_normal(W.sum()) + 1j * rng.standard_normal(W.sum())
+    g = np.zeros(data.op.No, dtype=complex)
+    g[W] = dr.dr_adjoint(H, lam, v)
+    assert np.allclose(Gdr.conj().T @ v, g)
+    # coupling stays within the 13 x 13 stencil of two 7 x 7 supports
+    Ky = data.op.Ky
+    idx = np.flatnonzero(W)
+    r, c = np.nonzero(np.abs(Hf) > 0)
+    d0 = (idx[c] % Ky - idx[r] % Ky + Ky // 2) % Ky - Ky // 2
+    d1 = (idx[c] // Ky - idx[r] // Ky + data.op.Kx // 2) % data.op.Kx - data.op.Kx // 2
+    assert np.abs(d0).max() <= 6 and np.abs(d1).max() <= 6
+
+
+def test_dr_reduced_data_and_dual_step():
+    """The DR dual step of update_dual_data_fidelity.m:85-125 (istril branch,
+    literal formulas) equals the oracle's l2-ball step on the DR data term."""
+    from oracle import dr
+    data, x, meta = problem.make_problem(16, 16, 2, 500, 2, seed=8, synth=synth)
+    ddr, ops = dr.dr_data_term(data)
+    rng = np.random.default_rng(3)
+    v2 = [[rng.standard_normal(len(b)) + 1j * rng.standard_normal(len(b)) for b in yl] for yl in ddr.y]
+    Fx_old = np.stack([data.op.A(0.7 * x[l]) for l in range(2)])
+    s22 = np.array([0.4, 0.3])
+    out = so.update_dual_data_fidelity(v2, 0.9 * x, Fx_old, ddr, s22)
+    for l, (H, W, lam) in enumerate(ops):
+        Fx = data.op.A(0.9 * x[l])
+        fp = 2 * Fx[W] - Fx_old[l][W]
+        z = v2[l][0] + dr.dr_forward(H, lam, fp) - ddr.y[l][0]
+        v2l = z * (1 - min(ddr.eps[l][0] / np.linalg.norm(z), 1))
+        assert np.allclose(out[0][l][0], v2l)
+        g2 = np.zeros(data.op.No, dtype=complex)
+        g2[W] = dr.dr_adjoint(H, lam, v2l)
+        assert np.allclose(out[1][l], s22[l] * np.real(data.op.At(g2)))
+        assert np.isclose(out[3][l][0], np.linalg.norm(dr.dr_forward(H, lam, Fx[W]) - ddr.y[l][0]))

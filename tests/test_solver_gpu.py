@@ -123,3 +123,21 @@ def test_fhs_iterations_match_golden_fixture():
     s.iterate(3)
     assert rel(np.moveaxis(s.x(), 2, 0), g["x3"]) < ITER_TOL
     s.close()
+
+
+def test_solver_destroy_after_operator():
+    """Destroying the operator before its solver (the order a garbage
+    collector may pick) leaves no CUDA error behind for later calls."""
+    from fhs_b200 import MeasurementOperator, Solver, proj_l2ball
+    from fhs_b200._lib import ALGO_HS
+    data, x, op, geom, nu2, sig, sig_bar = _setup("hs", L=2)
+    s = Solver(op, ALGO_HS, _params(nu2, sig, sig_bar))
+    s.set_data(data.y, data.eps)
+    s.init()
+    s.iterate(2)
+    op.close()
+    s.close()
+    op2 = MeasurementOperator(op.Ny, op.Nx, [(np.zeros(4), np.zeros(4))])
+    v = np.ones(8, dtype=complex)
+    assert np.allclose(proj_l2ball(v, 1.0, 0 * v), v / np.sqrt(8))
+    op2.close()
