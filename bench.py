@@ -160,6 +160,15 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
     P = sum(facet_pixels(sy, sx, (ov, ov)))
     s_w = sp_s - N
     pre = 20 if prob.get("precond") else 0
+    if prob.get("dr"):
+        # DR apply passes: the 85-entry c64 half stencil and the weight (c64)
+        # of the n active cells, the cell -> index map (i32) of every cell;
+        # pass 1 reads the half spectrum and y, v2, H Fx_old and writes z,
+        # H Fx; pass 2 reads z, writes v2 and the full gridded plane
+        n = op.n_vis_total
+        stencil = n * (85 * 8 + 8) + L * No * 4
+        dr_bytes = {"degrid_dual": stencil + L * (No // 2) * 8 + n * (8 + 8 + 8) + n * (8 + 8),
+                    "grid_dual": stencil + n * 8 + n * 8 + L * No * 8}
     out = {
         "primal_pad": N * L * (4 + 4) + N * L * (4 + 4 + 8),
         "degrid_dual": No * L * 8 + M * (16 + 8 + 8 + 8 + pre) + M * (8 + 8),
@@ -171,6 +180,8 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
         "facet_reconstruct": 3 * P * L * 4,
         "assemble_g": N * L * (8 + 4 + 4) + P * L * 4,
     }
+    if prob.get("dr"):
+        out.update(dr_bytes)
     if fb_counts is not None:
         out["ellipse_fb"] = sum(k * m * 53 for kl, bl in zip(fb_counts, op.block_sizes) for k, m in zip(kl, bl))
     return out
@@ -265,7 +276,7 @@ def run_ours(args):
     from fhs_b200.workload import build_problem, make_solver
     seed = 1000 + rank
     wl = {"small": SMALL, "medium": MEDIUM}.get(args.case, WORKLOAD)
-    prob = build_problem(**wl, seed=seed, device=local, precond=args.precond)
+    prob = build_problem(**wl, seed=seed, device=local, precond=args.precond, dr=args.dr)
     s = make_solver(prob)
     s.init()
     s.iterate(args.warmup, record=False)
@@ -293,7 +304,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                 "algorithmic_bytes": nbytes[dom], "ms_per_launch": mine[dom],
-                "traffic": _traffic_from_profiles(dom)}
+                "traffic": _traffic_from_profiles(("dr_" if args.dr else "") + dom)}
     stage_rows = {k: {"ms": round(v, 4), **({"gbs": round(nbytes[k] / (v / 1e3) / 1e9, 1)} if k in nbytes and v > 0
                                            else {})} for k, v in stages.items()}
     # ---- end to end through the public API with pinned host buffers
@@ -321,10 +332,15 @@ def run_ours(args):
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": _config({"visibilities": prob["n_vis"], "parallelism": f"{world} independent cubes"})
-                if args.case == "full" else {"workload": f"fhs_{wl['Ny']}x{wl['Nx']}x{wl['L']}_C4_Q4x4 (profiling case)"},
+                if args.case == "full" and not args.dr else
+                {"workload": f"fhs_{wl['Ny']}x{wl['Nx']}x{wl['L']}_C{wl.get('C', 4)}_Q4x4"
+                             + (" DR variant" if args.dr else " (profiling case)"),
+                 "visibilities": prob["n_vis"], "active_cells": prob["op"].n_vis_total if args.dr else None},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks, "stages_ms": stage_rows, "data_term": "ellipsoid projection, uniform-weight pU"
-                if args.precond else "l2 ball (pU = 1)",
+                if args.precond else ("visibility gridding (DR), l2 ball, 1 block per channel; stages "
+                                      "degrid_dual / grid_dual are the two DR stencil passes" if args.dr
+                                      else "l2 ball (pU = 1)"),
                 "vis_per_s": 2.0 * prob["n_vis"] * value}
         print(json.dumps(line), flush=True)
     s.close()
@@ -368,8 +384,12 @@ def main():
                     help="medium (512x512x64) / small (512x512x16): profiling cases for ncu captures, not bench lines")
     ap.add_argument("--precond", action="store_true",
                     help="variant: uniform-weight preconditioner and the ellipsoid projection (not the bench line)")
+    ap.add_argument("--dr", action="store_true",
+                    help="variant: visibility gridding (DR) of the same workload (not the bench line)")
     args = ap.parse_args()
-    if args.precond:
+    if args.precond and args.dr:
+        ap.error("the reference has no preconditioner with DR")
+    if args.precond or args.dr:
         args.no_cpu_baseline = True
     if args.warmup < 3:
         args.warmup = 3

@@ -16,20 +16,25 @@
 //
 // Two cells couple only when one visibility's 7 x 7 support holds both, so H
 // is a 13 x 13 stencil on the (periodic) oversampled grid.  It is stored as
-// its half T over the whole grid, [L][85][Kx][Ky] c64: T[k][0] = H_kk / 2 and
-// T[k][d] = H(k, k + d) for the 84 offsets with d1 < 0 or (d1 == 0, d0 < 0),
-// so that H u = T u + T^H u:
-//   (H u)[k] = 2 Re(T[k][0]) u[k] + sum_d T[k][d] u[k + d] + conj(T[k - d][d]) u[k - d].
-// The apply kernel is a gather (no atomics): a CTA stages u over a 64 x 16
-// cell tile and its 6-cell apron in shared memory and streams both T reads
-// of an offset back to back (the shifted one hits the lines just loaded).
+// its half T on the active cells only, per channel [85][n_c] c64 (plane j,
+// data index i): T[i][0] = H_kk / 2 and T[i][d] = H(k, k + d) for the 84
+// offsets with d1 < 0 or (d1 == 0, d0 < 0), so that H u = T u + T^H u:
+//   (H u)[k] = 2 Re(T[k][0]) u[k] + sum_d T[k][d] u[k + d] + conj(T[k - d][d]) u[k - d]
+// (rows of inactive cells are zero and not stored).  The apply kernel is a
+// gather (no atomics): a CTA stages u and the cell -> data index map over a
+// 64 x 16 cell tile and its 6-cell apron in shared memory; per offset each
+// thread loads T of its 4 cells and of their neighbours k - d (index from the
+// staged map) together, 8 independent loads in flight, since the kernel
+// waits on global-load latency.  Tiles without active cells skip the loop.
 // The data space of channel c is its active cells in column-major order, the
 // order of MATLAB's Fx(W); solver vectors (y, v2, G Fx_old, z) live there.
 //
-// H is built on the device in FP64 from the committed visibility operator:
-// one CTA per 8 x 8 cell block gathers the visibilities of the 2 x 2
-// sub-bins whose supports can reach the block, each thread owning a fixed
-// set of (cell, offset) sums (deterministic, no atomics).
+// H is built on the device in FP64 from the committed visibility operator,
+// one channel at a time into a dense [85][Ky Kx] scratch: one CTA per 8 x 8
+// cell block gathers the visibilities of the 2 x 2 sub-bins whose supports
+// can reach the block, each thread owning a fixed set of (cell, offset) sums
+// (deterministic, no atomics); the active rows are then gathered into the
+// compact store.
 #include <algorithm>
 #include <cmath>
 #include <numeric>
@@ -150,6 +155,14 @@ __global__ void __launch_bounds__(kBuildThreads) dr_build_kernel(OpView op, int 
   }
 }
 
+// compact store of one channel: Tc[j][i] = dense[j][cell_i]
+__global__ void dr_compact_kernel(const float2* __restrict__ dense, const int32_t* __restrict__ cells, int64_t n,
+                                  int64_t No, float2* __restrict__ Tc) {
+  const int j = blockIdx.y;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    Tc[j * n + i] = dense[j * No + cells[i]];
+}
+
 // ------------------------------------------------------------------ apply
 // MODE 0: out(W) = omega (H u), u = Fx.  MODE 1: l2-ball dual pass 1 (u = Fx;
 // hf = omega (H u), z = v2 + 2 hf - gold - y -> zbuf, hf -> gold, FP64 sums
@@ -157,12 +170,19 @@ __global__ void __launch_bounds__(kBuildThreads) dr_build_kernel(OpView op, int 
 // gridB = H u; v2 = scale z on W).  MODE 3: gridB = H u, u = conj(omega) vin.
 // HALF: u is read from the R2C half spectrum [Kx][Ky/2 + 1].
 struct DrView {
-  const float2* T;
+  const float2* const* T;  // [L] per-channel stencil [85][n_c]
   const float2* omega;
   const int32_t* map;
   const int64_t* ch_voff;
   const float* blk_scale;
+  const int32_t* ch_M;
   int Ky, Kx, tiles_y, tiles;
+};
+
+struct DrSmem {
+  float2 su[kDrSX][kDrSY];              // operand u over the tile and its 6-cell apron
+  int32_t sm[kDrSX][kDrSY];             // data index of each staged cell, -1 off W
+  double red[2][8];
 };
 
 template <int MODE, bool HALF>
@@ -171,8 +191,8 @@ __global__ void __launch_bounds__(256) dr_apply_kernel(DrView dv, int c0, const 
                                                        float2* __restrict__ gridB, float2* __restrict__ v2,
                                                        float2* __restrict__ gold, const float2* __restrict__ y,
                                                        float2* __restrict__ zbuf, double* __restrict__ partials) {
-  __shared__ float2 su[kDrSX][kDrSY];
-  __shared__ double red[2][8];
+  extern __shared__ __align__(16) unsigned char dr_smem_raw[];
+  DrSmem& S = *reinterpret_cast<DrSmem*>(dr_smem_raw);
   const int ch = c0 + blockIdx.y;
   const int tile = blockIdx.x;
   const int B0 = (tile % dv.tiles_y) * kDrTileY, B1 = (tile / dv.tiles_y) * kDrTileX;
@@ -182,12 +202,20 @@ __global__ void __launch_bounds__(256) dr_apply_kernel(DrView dv, int c0, const 
   const int32_t* map = dv.map + (size_t)ch * No;
   const int64_t vo = dv.ch_voff[ch];
   const float scale = MODE == 2 ? dv.blk_scale[(size_t)ch * kMaxBlocksPerChannel] : 1.f;
-  // stage u over the tile and its apron (periodic grid)
+  const int ty = threadIdx.x % kDrTileY, tx = threadIdx.x / kDrTileY;  // 4 column groups
+  const int k0 = B0 + ty;
+  // stage u and the index map over the tile and its apron (periodic grid)
   const int Kh = Ky / 2 + 1;
   const float2* g = gridA + (size_t)ch * (HALF ? Kh : Ky) * Kx;
+  int own = 0;
   for (int idx = threadIdx.x; idx < kDrSX * kDrSY; idx += blockDim.x) {
     const int cx = idx / kDrSY, cy = idx - cx * kDrSY;
     const int q0 = wrap(B0 - kDrReach + cy, Ky), q1 = wrap(B1 - kDrReach + cx, Kx);
+    const int64_t q = (int64_t)q1 * Ky + q0;
+    const int i = map[q];
+    S.sm[cx][cy] = i;
+    if (i >= 0 && cx >= kDrReach && cx < kDrReach + kDrTileX && cy >= kDrReach && cy < kDrReach + kDrTileY)
+      own = 1;
     float2 u;
     if (MODE <= 1) {
       if (!HALF) {
@@ -199,20 +227,55 @@ __global__ void __launch_bounds__(256) dr_apply_kernel(DrView dv, int c0, const 
         u = make_float2(m.x, -m.y);
       }
     } else {
-      const int64_t q = (int64_t)q1 * Ky + q0;
-      const int i = map[q];
       u = make_float2(0.f, 0.f);
       if (i >= 0) {
         const float2 z = MODE == 2 ? zbuf[vo + i] : vin[vo + i];
-        const float2 w = omega[q];
-        u = cmulc(w, make_float2(scale * z.x, scale * z.y));
+        u = cmulc(omega[q], make_float2(scale * z.x, scale * z.y));
       }
     }
-    su[cx][cy] = u;
+    S.su[cx][cy] = u;
   }
-  __syncthreads();
-  const int ty = threadIdx.x % kDrTileY, tx = threadIdx.x / kDrTileY;  // 4 column groups
-  const int k0 = B0 + ty;
+  own = __syncthreads_or(own);
+  float2 acc[kDrTileX / 4];
+#pragma unroll
+  for (int r = 0; r < kDrTileX / 4; ++r) acc[r] = make_float2(0.f, 0.f);
+  if (own) {
+    // per offset, the 4 cells of a thread issue their 8 stencil loads together
+    // (the kernel waits on global loads: memory-level parallelism per thread)
+    const int64_t n = dv.ch_M[ch];
+    const float2* Tc = dv.T[ch];
+    int ia[kDrTileX / 4];
+#pragma unroll
+    for (int r = 0; r < kDrTileX / 4; ++r) {
+      const int lx = tx + 4 * r;
+      ia[r] = S.sm[lx + kDrReach][ty + kDrReach];
+      if (ia[r] >= 0) {
+        const float2 t0 = __ldg(Tc + ia[r]);
+        const float2 uk = S.su[lx + kDrReach][ty + kDrReach];
+        acc[r] = make_float2(2.f * t0.x * uk.x, 2.f * t0.x * uk.y);
+      }
+    }
+#pragma unroll 2
+    for (int j = 1; j < kDrHalf; ++j) {
+      int d0, d1;
+      dr_offset(j, d0, d1);
+      const float2* Tj = Tc + j * n;
+      float2 a[kDrTileX / 4], b[kDrTileX / 4];
+#pragma unroll
+      for (int r = 0; r < kDrTileX / 4; ++r) {
+        const int lx = tx + 4 * r;
+        const int ib = S.sm[lx + kDrReach - d1][ty + kDrReach - d0];  // neighbour k - d
+        a[r] = ia[r] >= 0 ? __ldg(Tj + ia[r]) : make_float2(0.f, 0.f);
+        b[r] = ib >= 0 && ia[r] >= 0 ? __ldg(Tj + ib) : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int r = 0; r < kDrTileX / 4; ++r) {
+        const int lx = tx + 4 * r;
+        acc[r] = cfma(a[r], S.su[lx + kDrReach + d1][ty + kDrReach + d0], acc[r]);
+        acc[r] = cfma(make_float2(b[r].x, -b[r].y), S.su[lx + kDrReach - d1][ty + kDrReach - d0], acc[r]);
+      }
+    }
+  }
   double nz = 0.0, nr = 0.0;
 #pragma unroll
   for (int r = 0; r < kDrTileX / 4; ++r) {
@@ -220,32 +283,12 @@ __global__ void __launch_bounds__(256) dr_apply_kernel(DrView dv, int c0, const 
     const int k1 = B1 + lx;
     if (k0 >= Ky || k1 >= Kx) continue;
     const int64_t k = (int64_t)k1 * Ky + k0;
-    const int i = map[k];
-    float2 acc = make_float2(0.f, 0.f);
-    if (i >= 0) {
-      const float2* Tc = dv.T + (size_t)ch * kDrHalf * No;
-      const float2 t0 = __ldg(Tc + k);
-      const float2 uk = su[lx + kDrReach][ty + kDrReach];
-      acc = make_float2(2.f * t0.x * uk.x, 2.f * t0.x * uk.y);
-#pragma unroll 4
-      for (int j = 1; j < kDrHalf; ++j) {
-        int d0, d1;
-        dr_offset(j, d0, d1);
-        const float2* Tj = Tc + (size_t)j * No;
-        const float2 a = __ldg(Tj + k);
-        int m0 = k0 - d0, m1 = k1 - d1;  // d1 <= 0: m1 >= k1
-        m0 += m0 < 0 ? Ky : (m0 >= Ky ? -Ky : 0);
-        m1 += m1 >= Kx ? -Kx : 0;
-        const float2 b = __ldg(Tj + (int64_t)m1 * Ky + m0);
-        acc = cfma(a, su[lx + kDrReach + d1][ty + kDrReach + d0], acc);
-        acc = cfma(make_float2(b.x, -b.y), su[lx + kDrReach - d1][ty + kDrReach - d0], acc);
-      }
-    }
+    const int i = S.sm[lx + kDrReach][ty + kDrReach];
     if (MODE == 0) {
-      if (i >= 0) out[vo + i] = cmul(omega[k], acc);
+      if (i >= 0) out[vo + i] = cmul(omega[k], acc[r]);
     } else if (MODE == 1) {
       if (i >= 0) {
-        const float2 hf = cmul(omega[k], acc);
+        const float2 hf = cmul(omega[k], acc[r]);
         const float2 yv = y[vo + i], vv = v2[vo + i], go = gold[vo + i];
         const float2 z = make_float2(vv.x + 2.f * hf.x - go.x - yv.x, vv.y + 2.f * hf.y - go.y - yv.y);
         zbuf[vo + i] = z;
@@ -255,7 +298,7 @@ __global__ void __launch_bounds__(256) dr_apply_kernel(DrView dv, int c0, const 
         nr += (double)rr.x * rr.x + (double)rr.y * rr.y;
       }
     } else {
-      gridB[(size_t)ch * No + k] = acc;
+      gridB[(size_t)ch * No + k] = acc[r];  // exactly 0 off W
       if (MODE == 2 && i >= 0) {
         const float2 z = zbuf[vo + i];
         v2[vo + i] = make_float2(scale * z.x, scale * z.y);
@@ -270,16 +313,30 @@ __global__ void __launch_bounds__(256) dr_apply_kernel(DrView dv, int c0, const 
     }
     const int w = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
-      red[0][w] = nz;
-      red[1][w] = nr;
+      S.red[0][w] = nz;
+      S.red[1][w] = nr;
     }
     __syncthreads();
     if (threadIdx.x < 2) {
       double t = 0.0;
-      for (int q = 0; q < 8; ++q) t += red[threadIdx.x][q];
+      for (int q = 0; q < 8; ++q) t += S.red[threadIdx.x][q];
       partials[((size_t)ch * dv.tiles + tile) * kMaxBlocksPerChannel * 2 + threadIdx.x] = t;
     }
   }
+}
+
+template <int MODE, bool HALF>
+void dr_launch(dim3 grid, cudaStream_t s, const DrView& dv, int c0, const float2* gA, const float2* vin,
+               float2* out, float2* gB, float2* v2, float2* gold, const float2* y, float2* zb, double* pa) {
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr[dev]) {
+    FHS_CUDA(cudaFuncSetAttribute(dr_apply_kernel<MODE, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(DrSmem)));
+    attr[dev] = true;
+  }
+  dr_apply_kernel<MODE, HALF><<<grid, 256, sizeof(DrSmem), s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
 }
 
 }  // namespace
@@ -289,7 +346,8 @@ void launch_dr_apply(const MeasOp* op, int mode, int c0, int nc, const float2* v
   FHS_CHECK(op->dr, FHS_ERR_STATE, "not a dimensionality-reduced operator");
   if (nc <= 0) return;
   DrView dv;
-  dv.T = op->dr_T.p;
+  dv.T = op->dr_Tptr.p;
+  dv.ch_M = op->ch_M.p;
   dv.omega = op->dr_omega.p;
   dv.map = op->dr_map.p;
   dv.ch_voff = op->ch_voff.p;
@@ -306,21 +364,21 @@ void launch_dr_apply(const MeasOp* op, int mode, int c0, int nc, const float2* v
   switch (mode) {
     case 0:
       if (half)
-        dr_apply_kernel<0, true><<<grid, 256, 0, s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
+        dr_launch<0, true>(grid, s, dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
       else
-        dr_apply_kernel<0, false><<<grid, 256, 0, s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
+        dr_launch<0, false>(grid, s, dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
       break;
     case 1:
       if (half)
-        dr_apply_kernel<1, true><<<grid, 256, 0, s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
+        dr_launch<1, true>(grid, s, dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
       else
-        dr_apply_kernel<1, false><<<grid, 256, 0, s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
+        dr_launch<1, false>(grid, s, dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
       break;
     case 2:
-      dr_apply_kernel<2, false><<<grid, 256, 0, s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
+      dr_launch<2, false>(grid, s, dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
       break;
     default:
-      dr_apply_kernel<3, false><<<grid, 256, 0, s>>>(dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
+      dr_launch<3, false>(grid, s, dv, c0, gA, vin, out, gB, v2, gold, y, zb, pa);
       break;
   }
   count_launch();
@@ -360,19 +418,23 @@ MeasOp* measop_create_dr(const MeasOp* vis) {
     FHS_CUDA(cudaStreamSynchronize(vis->stream));
     op->dr = true;
     op->dr_tiles = ((op->Ky + kDrTileY - 1) / kDrTileY) * ((op->Kx + kDrTileX - 1) / kDrTileX);
-    op->dr_T.alloc((size_t)L * kDrHalf * No);
     op->dr_omega.alloc((size_t)L * No);
     op->dr_map.alloc((size_t)L * No);
+    op->dr_Tc.resize(L);
+    DevBuf<float2> dense;   // one channel's stencil over the whole grid
+    dense.alloc((size_t)kDrHalf * No);
     DevBuf<double> diag;
     diag.alloc((size_t)No);
+    DevBuf<int32_t> dcell;
     std::vector<double> hd((size_t)No);
     std::vector<float2> hl((size_t)No);
     std::vector<int32_t> hm((size_t)No);
     std::vector<int32_t> cells;
+    std::vector<float2*> tptr(L, nullptr);
     const OpView v = vis->view();
     for (int c = 0; c < L; ++c) {
       dim3 grid(vis->nsb0, vis->nsb1, 1);
-      dr_build_kernel<<<grid, kBuildThreads, 0, s>>>(v, c, op->dr_T.p + (size_t)c * kDrHalf * No, diag.p);
+      dr_build_kernel<<<grid, kBuildThreads, 0, s>>>(v, c, dense.p, diag.p);
       count_launch();
       FHS_LAUNCH_CHECK();
       diag.download(hd.data(), No, s);
@@ -381,6 +443,7 @@ MeasOp* measop_create_dr(const MeasOp* vis) {
       // (util_load_data_gen_dr_measurement_operator.m:213-216); omega = Lambda conj(rho)
       ChannelHost& h = op->ch[c];
       h.perm.clear();
+      const size_t first = cells.size();
       int32_t n = 0;
       for (int64_t k = 0; k < No; ++k) {
         if (hd[k] > 0) {
@@ -406,8 +469,21 @@ MeasOp* measop_create_dr(const MeasOp* vis) {
                                cudaMemcpyHostToDevice, s));
       FHS_CUDA(cudaMemcpyAsync(op->dr_map.p + (size_t)c * No, hm.data(), No * sizeof(int32_t),
                                cudaMemcpyHostToDevice, s));
+      if (n > 0) {
+        op->dr_Tc[c].reset(new DevBuf<float2>());
+        op->dr_Tc[c]->alloc((size_t)kDrHalf * n);
+        tptr[c] = op->dr_Tc[c]->p;
+        if (dcell.n < (size_t)n) dcell.alloc(n);
+        dcell.upload(cells.data() + first, n, s);
+        dim3 cg((unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), kDrHalf);
+        dr_compact_kernel<<<cg, 256, 0, s>>>(dense.p, dcell.p, n, No, tptr[c]);
+        count_launch();
+        FHS_LAUNCH_CHECK();
+      }
       FHS_CUDA(cudaStreamSynchronize(s));
     }
+    op->dr_Tptr.alloc(L);
+    op->dr_Tptr.upload(tptr.data(), L, s);
     op->dr_cell.alloc(std::max<size_t>(cells.size(), 1));
     op->dr_cell.upload(cells.data(), cells.size(), s);
     measop_commit(op);

@@ -1,6 +1,8 @@
 // Measurement operator Phi = G A on the device (see measop.cu).
 #pragma once
 
+#include <memory>
+
 #include "common.cuh"
 #include "minmax.h"
 
@@ -135,9 +137,10 @@ struct MeasOp {
   // dimensionality reduction (visibility gridding, measop_create_dr): the
   // data space of channel c is its active grid cells W_c (diag(G^H G) > 0) in
   // column-major order; the operator is Lambda H on W_c with H = G^H G kept as
-  // a half stencil T (diagonal halved, H = T + T^H) over the whole grid.
+  // a half stencil T (diagonal halved, H = T + T^H) on the active cells.
   bool dr = false;
-  DevBuf<float2> dr_T;      // [L][kDrHalf][Kx][Ky]
+  std::vector<std::unique_ptr<DevBuf<float2>>> dr_Tc;  // [L] half stencil [kDrHalf][n_c] of the active cells
+  DevBuf<float2*> dr_Tptr;  // [L] device copies of the dr_Tc pointers
   DevBuf<float2> dr_omega;  // [L][Kx][Ky] Lambda conj(rho): Lambda = diag(H)^-1/2 on W_c, 0 elsewhere
   DevBuf<int32_t> dr_map;   // [L][Kx][Ky] data index (channel-relative) of each cell, -1 off W_c
   DevBuf<int32_t> dr_cell;  // [Mtot] grid cell of each data entry

@@ -21,9 +21,13 @@ from .api import HS_forward_operator_G, MeasurementOperator, Solver, gen_precond
 
 def build_problem(Ny=1024, Nx=1024, L=64, C=4, Q=4, overlap_frac=0.1, jitter=0.15, m_lo=0.3, m_hi=1.0,
                   blocks=(2, 6), snr_db=40.0, seed=0, device=0, opnorm_iter=50, opnorm_tol=1e-6,
-                  pdfb_max_iter=2000, reweighting_max_iter=20, precond=False):
+                  pdfb_max_iter=2000, reweighting_max_iter=20, precond=False, dr=False):
     """``precond``: attach the uniform-weight preconditioner (the reference's
-    default data term) and take nu2 from the preconditioned operator norm."""
+    default data term) and take nu2 from the preconditioned operator norm.
+    ``dr``: visibility gridding (util_load_data_gen_dr_measurement_operator.m):
+    the solver runs on the DR operator, with the gridded data and the l2
+    bounds of gridded unit-variance (whitened) noise; the visibility operator
+    is released once the data are reduced."""
     rng = np.random.default_rng(seed)
     N = Ny * Nx
     lg = L // C
@@ -60,6 +64,14 @@ def build_problem(Ny=1024, Nx=1024, L=64, C=4, Q=4, overlap_frac=0.1, jitter=0.1
     op = MeasurementOperator(Ny, Nx, om, bsz, [np.full(len(o[0]), 1.0 / s) for o, s in zip(om, sig)],
                              device=device)
     eps = [synth.l2_bounds(b) for b in bsz]
+    n_vis = int(sum(Ms))
+    if dr:
+        dop = op.dimensionality_reduction()
+        y = op.reduce_data(dop, y)
+        noise = [synth.noise(int(sum(b)), rng) for b in bsz]
+        eps = [[float(np.linalg.norm(v[0]))] for v in op.reduce_data(dop, noise)]
+        op.close()
+        op = dop
     if precond:
         op.set_preconditioner([gen_preconditioning_matrix(oy, ox, op.Ky, op.Kx) for oy, ox in om])
     nu2 = op.operator_norm(opnorm_iter, opnorm_tol, precond=precond)
@@ -77,7 +89,7 @@ def build_problem(Ny=1024, Nx=1024, L=64, C=4, Q=4, overlap_frac=0.1, jitter=0.1
     param = dict(nu2=nu2, gamma=gam, gamma0=gam0, reweighting_sig=rs, reweighting_sig_bar=rsb,
                  pdfb_max_iter=pdfb_max_iter, reweighting_max_iter=reweighting_max_iter)
     return dict(op=op, y=y, eps=eps, x_true=x_int, param=param, splits=(sy, sx), overlap=(ov, ov), C=C, Q=Q,
-                order=order, n_vis=int(sum(Ms)), nu2=nu2, precond=precond)
+                order=order, n_vis=n_vis, nu2=nu2, precond=precond, dr=dr)
 
 
 def make_solver(prob, nlevel=4):
