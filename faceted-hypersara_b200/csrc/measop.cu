@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
           st[lane * 2 * J + j] = make_float2(hy[j].x, -hy[j].y);   // conj(hy)
           st[lane * 2 * J + J + j] = cmulc(hx[j], v);               // conj(hx) w v
         }
-        sd[lane] = make_int2(d0, d1 - xb);
+        sd[lane] = make_int2((d1 - xb) * kAccPitch + d0, d0);
       }
       __syncwarp();
       // Taps outside the tile need no test: columns left of the tile (band 0)
@@ -354,44 +354,18 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
       // ring above the tile (part 1) reaches negative rows, which are skipped.
       if (part == 0) {
         for (int k = 0; k < n; ++k) {
-          const int2 d = sd[k];                 // (row offset, band column offset)
+          const int a = sd[k].x;                // accumulator index of tap (0, 0)
           const float2* sk = st + k * 2 * J;
-          const int a = d.y * kAccPitch + d.x;  // accumulator index of tap (0, 0)
-          {
-            const float2 val = cmul(sk[jyA], sk[J + jxA]);
-            float2 o = ab[a + offA];
-            o.x += val.x;
-            o.y += val.y;
-            ab[a + offA] = o;
-          }
-          if (hasB) {
-            const float2 val = cmul(sk[jyB], sk[J + jxB]);
-            float2 o = ab[a + offB];
-            o.x += val.x;
-            o.y += val.y;
-            ab[a + offB] = o;
-          }
+          ab[a + offA] = cfma(sk[jyA], sk[J + jxA], ab[a + offA]);
+          if (hasB) ab[a + offB] = cfma(sk[jyB], sk[J + jxB], ab[a + offB]);
           __syncwarp();
         }
       } else {
         for (int k = 0; k < n; ++k) {
-          const int2 d = sd[k];
+          const int2 d = sd[k];                 // (accumulator index, row offset)
           const float2* sk = st + k * 2 * J;
-          const int a = d.y * kAccPitch + d.x;
-          if (d.x + jyA >= 0) {
-            const float2 val = cmul(sk[jyA], sk[J + jxA]);
-            float2 o = ab[a + offA];
-            o.x += val.x;
-            o.y += val.y;
-            ab[a + offA] = o;
-          }
-          if (hasB && d.x + jyB >= 0) {
-            const float2 val = cmul(sk[jyB], sk[J + jxB]);
-            float2 o = ab[a + offB];
-            o.x += val.x;
-            o.y += val.y;
-            ab[a + offB] = o;
-          }
+          if (d.y + jyA >= 0) ab[d.x + offA] = cfma(sk[jyA], sk[J + jxA], ab[d.x + offA]);
+          if (hasB && d.y + jyB >= 0) ab[d.x + offB] = cfma(sk[jyB], sk[J + jxB], ab[d.x + offB]);
           __syncwarp();
         }
       }
