@@ -12,6 +12,7 @@
 //   FP64 statistics into a device ring (rel_x, ||x||, residual, eps, priors).
 // The host reads the ring once per iteration only when it evaluates the
 // stopping rule (facetHyperSARA.m:877-881) and reweights (:952-1137).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <memory>
@@ -499,6 +500,7 @@ fhs_status fhs_solver_set_data(fhs_solver* s_, const double* y, const double* ep
         e[(size_t)l * kMaxBlocksPerChannel + b] = v;
       }
     op->blk_eps.upload(e.data(), e.size(), s);
+    S->h_eps.assign(eps, eps + op->nblk_tot);
     FHS_CUDA(cudaStreamSynchronize(s));
     S->data_set = true;
   });
@@ -543,7 +545,16 @@ fhs_status fhs_solver_set_params(fhs_solver* s_, const fhs_solver_params* p) {
       S->fb_min = 1;
       S->fb_stop = 1e-8;
     }
+    S->adjust_noise = p->adjust_flag_noise != 0 && S->algo != FHS_ALGO_SARA;
+    S->adjust_min_iter = p->adjust_noise_min_iter > 0 ? p->adjust_noise_min_iter : 100;
+    S->adjust_rel_var = p->adjust_noise_rel_var > 0 ? p->adjust_noise_rel_var : 1e-3;
+    S->adjust_start_iter = p->adjust_noise_start_iter > 0 ? p->adjust_noise_start_iter : 2000;
+    S->adjust_change = p->adjust_noise_change_percentage > 0 ? p->adjust_noise_change_percentage : 0.5;
+    S->alph = p->alph > 0 ? p->alph : 1.0;
+    S->alph_bar = p->alph_bar > 0 ? p->alph_bar : 1.0;
     const double sigma0 = 1.0 / p->nu0, sigma1 = 1.0 / p->nu1;
+    S->sigma0 = sigma0;
+    S->sigma1 = sigma1;
     // facetHyperSARA.m:582-608 / hyperSARA.m:471-487: tau = 0.99/3;
     // sara.m:502-505: tau = 0.99/(sigma1 nu1 + sigma2 nu2) = 0.99/2
     S->tau = S->algo == FHS_ALGO_SARA ? 0.99 / 2.0 : 0.99 / 3.0;
@@ -680,6 +691,70 @@ fhs_status fhs_solver_update_weights(fhs_solver* s_) {
   });
 }
 
+// beta1 = gamma / sigma1, beta0 = gamma0 / sigma0 from the host copies (or 0:
+// priors off, facetHyperSARA.m:704-708)
+static void upload_betas(Solver* S, bool off) {
+  cudaStream_t s = S->op->stream;
+  const int G = S->G;
+  std::vector<double> b1(G);
+  for (int g = 0; g < G; ++g) b1[g] = off ? 0.0 : S->gamma[g] / S->sigma1;
+  S->beta1.upload(b1.data(), G, s);
+  if (S->nuclear) {
+    std::vector<double> b0(S->gamma0.size());
+    for (size_t i = 0; i < b0.size(); ++i) b0[i] = off ? 0.0 : S->gamma0[i] / S->sigma0;
+    S->beta0.upload(b0.data(), b0.size(), s);
+  }
+  FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+// facetHyperSARA.m:903-937 / hyperSARA.m:697-731: adapts the l2 bounds from
+// the last block residuals, re-estimates the channel noise levels and sets
+// gamma / gamma0 from compute_noise_level.m:49-89 (FP64, host).
+static void adjust_noise_level(Solver* S) {
+  MeasOp* op = S->op;
+  cudaStream_t s = op->stream;
+  std::vector<double> st((size_t)op->nblk_tot * 2);
+  op->blk_stats.download(st.data(), st.size(), s);
+  FHS_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> e((size_t)op->L * kMaxBlocksPerChannel, 0.0), sig_ch(op->L, 0.0);
+  for (int l = 0; l < op->L; ++l) {
+    double e2 = 0.0, m = 0.0;
+    for (int b = 0; b < op->h_nblk[l]; ++b) {
+      const int gb = op->h_blkoff[l] + b;
+      const double r = std::sqrt(st[2 * gb + 1]);
+      double& eps = S->h_eps[gb];
+      if (eps < (2.0 - S->pdfb_tol) * r) eps = (eps + r) * S->adjust_change;
+      e[(size_t)l * kMaxBlocksPerChannel + b] = eps;
+      e2 += eps * eps;
+      m += (double)op->ch[l].block_sizes[b];
+    }
+    // expectation of std() of the reference's randn draw with per-block
+    // variance eps_b^2 / M_b
+    sig_ch[l] = m > 0 ? std::sqrt(e2 / m) : 0.0;
+  }
+  op->blk_eps.upload(e.data(), e.size(), s);
+  const int lg = S->lg;
+  const double mu_chi = std::sqrt(2.0) * std::exp(std::lgamma((lg + 1) / 2.0) - std::lgamma(lg / 2.0));
+  const double sig_chi = std::sqrt(std::max(lg - mu_chi * mu_chi, 0.0));
+  for (int g = 0; g < S->G; ++g) {
+    double ssum = 0.0;
+    for (int i = 0; i < lg; ++i) {
+      const int l = g * lg + i;
+      ssum += sig_ch[l] * sig_ch[l] / S->nu2[l];
+    }
+    const double sig_sara = std::sqrt(ssum / lg);
+    S->gamma[g] = S->alph * sig_sara * (mu_chi + sig_chi);
+    if (S->nuclear) {
+      for (int q = 0; q < S->np.Q; ++q) {
+        const NucFacet& f = S->np.facets[q];
+        const double P = (double)(f.y1 - f.y0) * (double)(f.x1 - f.x0);
+        S->gamma0[(size_t)g * S->np.Q + q] = S->alph_bar * std::sqrt(P * ssum / std::min(P, (double)lg));
+      }
+    }
+  }
+  upload_betas(S, false);
+}
+
 fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
   return guarded_solver([&] {
     Solver* S = sv(s_);
@@ -696,8 +771,10 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
     const int nb = nblk(n);
     dn.alloc(2 * nb);
     std::vector<double> hdn(2 * nb), rec;
-    int last = 0, rw_count = 0, t = 0, converged = 0;
+    int last = 0, rw_count = 0, t = 0, converged = 0, n_adjust = 0;
     fhs_iter_info info{};
+    bool adjust = S->adjust_noise;
+    if (adjust) upload_betas(S, true);  // priors off until the first adjustment
     for (t = 1; t <= max_iter; ++t) {
       FHS_CUDA(cudaGraphLaunch(S->graph, s));
       g_launches += S->launches_per_iter;
@@ -710,7 +787,20 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
                         (t - last >= S->pdfb_max ||
                          (info.rel_val <= S->pdfb_rel_var && info.residual <= S->pdfb_tol * info.epsilon) ||
                          info.rel_val <= S->pdfb_rel_var_low);
+      if (adjust && info.residual > S->pdfb_tol * info.epsilon) {
+        // facetHyperSARA.m:883-889 (also at the run's first iteration) /
+        // hyperSARA.m:690-695 (at adjust_noise_start_iter instead)
+        const bool early = S->algo == FHS_ALGO_FHS ? last < 1 : (last < 1 && t == S->adjust_start_iter);
+        if (t - last >= S->pdfb_max || early ||
+            (info.rel_val <= S->adjust_rel_var && t - last >= S->adjust_min_iter)) {
+          adjust_noise_level(S);
+          ++n_adjust;
+          last = t;
+          continue;
+        }
+      }
       if (!pdfb) continue;
+      adjust = false;  // facetHyperSARA.m:952
       diff_norm_kernel<<<nb, 256, 0, s>>>(x_rw.p, S->x.p, n, dn.p);
       count_launch();
       FHS_LAUNCH_CHECK();
@@ -740,6 +830,7 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
       out->residual = info.residual;
       out->epsilon = info.epsilon;
       out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      out->n_noise_adjustments = n_adjust;
     }
   });
 }
@@ -757,6 +848,25 @@ fhs_status fhs_solver_ellipse_iterations(fhs_solver* s_, int* counts) {
     }
     for (int l = 0; l < op->L; ++l)
       for (int b = 0; b < op->h_nblk[l]; ++b) counts[op->h_blkoff[l] + b] = c[(size_t)l * kMaxBlocksPerChannel + b];
+  });
+}
+
+fhs_status fhs_solver_epsilon(fhs_solver* s_, double* epsilon) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(epsilon != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    FHS_CHECK(S->data_set, FHS_ERR_STATE, "no data set");
+    std::copy(S->h_eps.begin(), S->h_eps.end(), epsilon);
+  });
+}
+
+fhs_status fhs_solver_regularization(fhs_solver* s_, double* gamma, double* gamma0) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(gamma != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    FHS_CHECK(S->params_set, FHS_ERR_STATE, "no parameters set");
+    std::copy(S->gamma.begin(), S->gamma.end(), gamma);
+    if (gamma0 && S->nuclear) std::copy(S->gamma0.begin(), S->gamma0.end(), gamma0);
   });
 }
 

@@ -43,6 +43,12 @@ struct Solver {
   double rw_rel_var = 1e-4;
   int pdfb_min = 10, pdfb_max = 2000;
   double pdfb_rel_var = 5e-5, pdfb_tol = 1.01, pdfb_rel_var_low = 5e-6;
+  double sigma0 = 1.0, sigma1 = 1.0;
+  // noise-level adjustment (fhs_solver_run)
+  bool adjust_noise = false;
+  int adjust_min_iter = 100, adjust_start_iter = 2000;
+  double adjust_rel_var = 1e-3, adjust_change = 0.5, alph = 1.0, alph_bar = 1.0;
+  std::vector<double> h_eps;     // [nblk_tot] current l2 bounds
   bool params_set = false, data_set = false, initialised = false;
 
   cudaGraphExec_t graph = nullptr;

@@ -44,7 +44,10 @@ class SolverParams(C.Structure):
                 ("pdfb_max_iter", C.c_int), ("pdfb_rel_var", C.c_double),
                 ("pdfb_fidelity_tolerance", C.c_double), ("pdfb_rel_var_low", C.c_double),
                 ("elipse_proj_max_iter", C.c_int), ("elipse_proj_min_iter", C.c_int),
-                ("elipse_proj_eps", C.c_double)]
+                ("elipse_proj_eps", C.c_double), ("adjust_flag_noise", C.c_int),
+                ("adjust_noise_min_iter", C.c_int), ("adjust_noise_rel_var", C.c_double),
+                ("adjust_noise_start_iter", C.c_int), ("adjust_noise_change_percentage", C.c_double),
+                ("alph", C.c_double), ("alph_bar", C.c_double)]
 
 
 class IterInfo(C.Structure):
@@ -55,7 +58,7 @@ class IterInfo(C.Structure):
 class RunInfo(C.Structure):
     _fields_ = [("n_iter", C.c_int), ("n_reweights", C.c_int), ("converged", C.c_int),
                 ("rel_val", C.c_double), ("residual", C.c_double), ("epsilon", C.c_double),
-                ("seconds", C.c_double)]
+                ("seconds", C.c_double), ("n_noise_adjustments", C.c_int)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -112,6 +115,8 @@ SIGNATURES = {
     "fhs_solver_get_x": (C.c_int, [_vp, _dp]),
     "fhs_solver_update_weights": (C.c_int, [_vp]),
     "fhs_solver_ellipse_iterations": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "fhs_solver_epsilon": (C.c_int, [_vp, _dp]),
+    "fhs_solver_regularization": (C.c_int, [_vp, _dp, _dp]),
     "fhs_solver_field_size": (C.c_int64, [_vp, C.c_int]),
     "fhs_solver_get_field": (C.c_int, [_vp, C.c_int, _dp]),
     "fhs_solver_set_field": (C.c_int, [_vp, C.c_int, _dp]),

@@ -416,7 +416,9 @@ _PARAM_DEFAULTS = dict(
     nu0=1.0, nu1=1.0, reweighting_alpha=1.0, reweighting_flag=True, reweighting_min_iter=1,
     reweighting_max_iter=20, reweighting_rel_var=1e-4, pdfb_min_iter=10, pdfb_max_iter=2000,
     pdfb_rel_var=5e-5, pdfb_fidelity_tolerance=1.01, pdfb_rel_var_low=5e-6,
-    elipse_proj_max_iter=20, elipse_proj_min_iter=1, elipse_proj_eps=1e-8)
+    elipse_proj_max_iter=20, elipse_proj_min_iter=1, elipse_proj_eps=1e-8,
+    adjust_flag_noise=False, adjust_noise_min_iter=100, adjust_noise_rel_var=1e-3,
+    adjust_noise_start_iter=2000, adjust_noise_change_percentage=0.5, alph=1.0, alph_bar=1.0)
 
 
 class Solver:
@@ -485,6 +487,12 @@ class Solver:
         sp.elipse_proj_max_iter = int(p["elipse_proj_max_iter"])
         sp.elipse_proj_min_iter = int(p["elipse_proj_min_iter"])
         sp.elipse_proj_eps = float(p["elipse_proj_eps"])
+        sp.adjust_flag_noise = int(bool(p["adjust_flag_noise"]))
+        sp.adjust_noise_min_iter = int(p["adjust_noise_min_iter"])
+        sp.adjust_noise_rel_var = float(p["adjust_noise_rel_var"])
+        sp.adjust_noise_start_iter = int(p["adjust_noise_start_iter"])
+        sp.adjust_noise_change_percentage = float(p["adjust_noise_change_percentage"])
+        sp.alph, sp.alph_bar = float(p["alph"]), float(p["alph_bar"])
         check(lib().fhs_solver_set_params(self._h, C.byref(sp)))
 
     def set_data(self, y, epsilon):
@@ -511,7 +519,25 @@ class Solver:
         ri = LB.RunInfo()
         check(lib().fhs_solver_run(self._h, int(max_iter), C.byref(ri)))
         return dict(n_iter=ri.n_iter, n_reweights=ri.n_reweights, converged=bool(ri.converged),
-                    rel_val=ri.rel_val, residual=ri.residual, epsilon=ri.epsilon, seconds=ri.seconds)
+                    rel_val=ri.rel_val, residual=ri.residual, epsilon=ri.epsilon, seconds=ri.seconds,
+                    n_noise_adjustments=ri.n_noise_adjustments)
+
+    def epsilon(self):
+        """Current l2 bounds as [l][b] (adapted by the noise adjustment of run())."""
+        out = np.empty(sum(len(b) for b in self.op.block_sizes))
+        check(lib().fhs_solver_epsilon(self._h, dptr(out)))
+        res, pos = [], 0
+        for bl in self.op.block_sizes:
+            res.append(list(out[pos:pos + len(bl)]))
+            pos += len(bl)
+        return res
+
+    def regularization(self):
+        """Current (gamma[groups], gamma0[groups x facets] or None)."""
+        g = np.empty(self.G)
+        g0 = np.empty(max(self.G * self.Q, 1))
+        check(lib().fhs_solver_regularization(self._h, dptr(g), dptr(g0) if self.Q else None))
+        return g, (g0 if self.Q else None)
 
     def update_weights(self):
         check(lib().fhs_solver_update_weights(self._h))

@@ -52,3 +52,26 @@ def compute_noise_level(Ny, Nx, n_channels, std_noise, algo, squared_operator_no
 def compute_noise_level_sara(std_noise, squared_operator_norm):
     """src/heuristics/compute_noise_level_sara.m:20."""
     return float(np.sqrt(float(std_noise) ** 2 / float(squared_operator_norm)))
+
+
+def update_epsilon(epsilon, t, t_block, norm_res, adapt_eps_tol_in, adapt_eps_tol_out, adapt_eps_steps,
+                   adapt_eps_change_percentage):
+    """src/update_epsilon.m:52-71 (adaptive l2 bounds, the reference's
+    use_adapt_eps; its solvers keep the call commented out): for every block
+    last changed more than adapt_eps_steps iterations ago, move eps towards
+    the residual, eps <- c ||res|| + (1 - c) eps, when ||res|| < tol_in eps
+    or ||res|| > tol_out eps.  epsilon, t_block, norm_res: [l][b] lists
+    (updated copies returned as (epsilon, t_block))."""
+    eps = [list(map(float, e)) for e in epsilon]
+    tb = [list(map(int, b)) for b in t_block]
+    c = float(adapt_eps_change_percentage)
+    for i, (el, rl) in enumerate(zip(eps, norm_res)):
+        for j, r in enumerate(rl):
+            if t > tb[i][j] + adapt_eps_steps:
+                if r < adapt_eps_tol_in * el[j]:
+                    el[j] = c * r + (1.0 - c) * el[j]
+                    tb[i][j] = t
+                if r > adapt_eps_tol_out * el[j]:
+                    el[j] = c * r + (1.0 - c) * el[j]
+                    tb[i][j] = t
+    return eps, tb

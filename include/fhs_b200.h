@@ -255,6 +255,21 @@ typedef struct fhs_solver_params {
    * elipse_proj_max_iter <= 0 selects 20 / 1 / 1e-8 for all three */
   int elipse_proj_max_iter, elipse_proj_min_iter;
   double elipse_proj_eps;
+  /* noise-level adjustment of fhs_solver_run (facetHyperSARA.m:503-526,
+   * 883-951; hyperSARA.m:406-429, 690-737; off in imaging/default_parameters.json):
+   * priors off from the run's first iteration until the first adjustment;
+   * an adjustment raises eps_b to (eps_b + ||res_b||) change_percentage where
+   * eps_b < (2 - pdfb_fidelity_tolerance) ||res_b||, re-estimates the
+   * channel noise sigma_l = sqrt(sum_b eps_b^2 / M_l) (the expectation of the
+   * reference's randn-based std) and sets gamma = alph sig, gamma0 =
+   * alph_bar sig_bar from compute_noise_level.  Values <= 0 select the
+   * reference defaults 100 / 1e-3 / 2000 / 0.5 / 1 / 1.  Not used by SARA. */
+  int adjust_flag_noise;
+  int adjust_noise_min_iter;
+  double adjust_noise_rel_var;
+  int adjust_noise_start_iter;
+  double adjust_noise_change_percentage;
+  double alph, alph_bar;
 } fhs_solver_params;
 
 /* Per-iteration record (FP64), summed over all groups. */
@@ -271,6 +286,7 @@ typedef struct fhs_run_info {
   int converged;
   double rel_val, residual, epsilon;
   double seconds;
+  int n_noise_adjustments;
 } fhs_run_info;
 
 typedef struct fhs_solver fhs_solver;
@@ -300,6 +316,12 @@ FHS_API fhs_status fhs_solver_get_x(fhs_solver* s, double* x);
  * The reference's solver_proj_elipse_fb returns the same count as its second
  * output (src/sara/sara.m:561). */
 FHS_API fhs_status fhs_solver_ellipse_iterations(fhs_solver* s, int* counts);
+/* Current l2 bounds, one per block (channel-major): the values given to
+ * set_data, or as adapted by the noise adjustment of fhs_solver_run. */
+FHS_API fhs_status fhs_solver_epsilon(fhs_solver* s, double* epsilon);
+/* Current regularisation parameters gamma[groups] and gamma0[groups x facets]
+ * (gamma0 may be NULL; ignored for SARA). */
+FHS_API fhs_status fhs_solver_regularization(fhs_solver* s, double* gamma, double* gamma0);
 
 /* Solver state for checkpoints and warm restarts: the arrays the reference
  * saves in its checkpoint files (src/fhs/facetHyperSARA.m:1071-1107: xsol, g,

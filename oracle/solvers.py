@@ -328,6 +328,14 @@ class SolverParams:
     pdfb_fidelity_tolerance: float = 1.01
     pdfb_rel_var_low: float = 5e-6
     nlevel: int = 4
+    # noise-level adjustment (facetHyperSARA.m:503-526, 877-951)
+    adjust_flag_noise: bool = False
+    adjust_noise_min_iter: int = 100
+    adjust_noise_rel_var: float = 1e-3
+    adjust_noise_start_iter: int = 2000
+    adjust_noise_change_percentage: float = 0.5
+    alph: float = 1.0
+    alph_bar: float = 1.0
 
 
 @dataclass
@@ -359,15 +367,43 @@ class Precond:
 
 def _dual_step(v2, proj, x, Fx_old, data, sigma22, pc: Precond | None):
     if pc is None:
-        v2, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, sigma22)
-        return v2, proj, Ftx, Fx_old, gres, geps
-    v2, proj, Ftx, Fx_old, _, gres, geps = update_dual_data_fidelity_precond(
+        v2, Ftx, Fx_old, nres, gres, geps = update_dual_data_fidelity(v2, x, Fx_old, data, sigma22)
+        return v2, proj, Ftx, Fx_old, gres, geps, nres
+    v2, proj, Ftx, Fx_old, nres, gres, geps = update_dual_data_fidelity_precond(
         v2, proj, x, Fx_old, data, pc.pU, sigma22, pc.max_itr, pc.min_itr, pc.stop)
-    return v2, proj, Ftx, Fx_old, gres, geps
+    return v2, proj, Ftx, Fx_old, gres, geps, nres
+
+
+def adjust_noise_trigger(algo, t, last, rel, res, epsn, p: SolverParams):
+    """pdfb_adjust_noise of facetHyperSARA.m:883-889 ('fhs': also at the
+    first iteration of the run) and hyperSARA.m:690-695 ('hs': at
+    adjust_noise_start_iter instead)."""
+    if not (res > p.pdfb_fidelity_tolerance * epsn):
+        return False
+    early = last < 1 if algo == "fhs" else (last < 1 and t == p.adjust_noise_start_iter)
+    return (t - last >= p.pdfb_max_iter or early
+            or (rel <= p.adjust_noise_rel_var and t - last >= p.adjust_noise_min_iter))
+
+
+def adjust_noise(eps, norm_res, block_sizes, p: SolverParams):
+    """facetHyperSARA.m:906-920: eps_b <- (eps_b + ||res_b||) c where
+    eps_b < (2 - tol) ||res_b||, then the channel noise level.  The reference
+    takes std() of a fresh randn draw with per-block sigma^2 = eps_b^2 / M_b;
+    this returns its expectation sqrt(sum_b eps_b^2 / sum_b M_b) (the draw
+    scatters around it by ~1/sqrt(2 M)).  Returns (eps, sigma per channel)."""
+    out, sig = [], []
+    for el, rl, ml in zip(eps, norm_res, block_sizes):
+        e = [(eb + rb) * p.adjust_noise_change_percentage
+             if eb < (2.0 - p.pdfb_fidelity_tolerance) * rb else eb for eb, rb in zip(el, rl)]
+        out.append(e)
+        m = float(sum(ml))
+        sig.append(float(np.sqrt(sum(v * v for v in e) / m)) if m > 0 else 0.0)
+    return out, np.array(sig)
 
 
 def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
-                    xinit=None, max_iter=None, callback=None, precond: Precond | None = None):
+                    xinit=None, max_iter=None, callback=None, precond: Precond | None = None,
+                    algo: str = "fhs"):
     """src/fhs/facetHyperSARA.m:701-1138 (one spectral sub-cube); proj starts
     at zero (src/fhs/fhs_initialize_data_worker.m:43)."""
     op = data.op
@@ -399,9 +435,15 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
     x_last_rw = x.copy()
     last, rw_count = 0, 0
     max_iter = max_iter or (p.reweighting_max_iter + 1) * p.pdfb_max_iter
+    adjust = bool(p.adjust_flag_noise)
+    if adjust:
+        # the l2 bounds change: work on a copy; priors off from the first
+        # iteration until the first adjustment (facetHyperSARA.m:704-708)
+        data = DataTerm(data.op, data.G, data.y, [list(e) for e in data.eps])
+        beta0, beta1 = np.zeros(geom.Q), 0.0
     for t in range(1, max_iter + 1):
         x, xhat, rel_x, norm_x = primal_update(x, g)
-        v2, proj, Ftx, Fx_old, gres, geps = _dual_step(v2, proj, x, Fx_old, data, sigma22, precond)
+        v2, proj, Ftx, Fx_old, gres, geps, nres = _dual_step(v2, proj, x, Fx_old, data, sigma22, precond)
         gacc = np.zeros_like(x)
         for q, (y0, y1), (x0, x1), win in facets:
             v0[q], g0 = nuclear_prox_update(v0[q], xhat[:, y0:y1, x0:x1], win, w0[q], beta0[q])
@@ -416,7 +458,19 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
         log.n_iter = t
         if callback is not None:
             callback(t, x)
+        if adjust and adjust_noise_trigger(algo, t, last, rel, res, epsn, p):
+            # facetHyperSARA.m:903-944 / hyperSARA.m:697-733
+            eps_new, sig_ch = adjust_noise(data.eps, nres, [[len(yb) for yb in yl] for yl in data.y], p)
+            data.eps[:] = eps_new
+            sig_n, sig_bar_n, *_ = compute_noise_level(op.Ny, op.Nx, L, sig_ch, algo,
+                                                       geom if algo == "fhs" else None, p.nu2)
+            beta1 = p.alph * sig_n / sigma1
+            beta0 = p.alph_bar * np.asarray(sig_bar_n, dtype=np.float64) * np.ones(geom.Q) / sigma0
+            log.n_adjust = getattr(log, "n_adjust", 0) + 1
+            last = t
+            continue
         if _stop_pdfb(t, last, rel, res, epsn, p):
+            adjust = False
             rel_rw = np.linalg.norm(x_last_rw - x) / max(np.linalg.norm(x_last_rw), 1e-300)
             if (not p.reweighting_flag) or (rw_count >= p.reweighting_min_iter and (
                     rw_count >= p.reweighting_max_iter or rel_rw <= p.reweighting_rel_var)):
@@ -428,6 +482,7 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
             rw_count += 1
             last = t
     log.n_reweights = rw_count
+    log.epsilon_final = [list(e) for e in data.eps]
     return x, log
 
 
@@ -439,7 +494,7 @@ def hypersara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callba
     # HyperSARA is the Q = 1 faceted iteration without window; its g0 scaling
     # (sigma0 inside hs_update_dual_lowrankness_serial.m:42) equals sigma00
     # because hyperSARA.m:476 also builds sigma00 = tau*sigma0.
-    return facet_hypersara(data, p, geom, xinit, max_iter, callback, precond)
+    return facet_hypersara(data, p, geom, xinit, max_iter, callback, precond, algo="hs")
 
 
 def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None,
@@ -475,7 +530,7 @@ def sara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=No
         r1 = v1 + wv.sara_analysis(xhat[0], p.nlevel)                # run_par_waverec
         v1 = r1 - np.sign(r1) * np.maximum(np.abs(r1) - beta1 * w1, 0.0)
         g1 = wv.sara_synthesis(v1, op.Ny, op.Nx, p.nlevel)
-        v2, proj, Ftx, Fx_old, gres, geps = _dual_step(v2, proj, x, Fx_old, data, [1.0], precond)
+        v2, proj, Ftx, Fx_old, gres, geps, _ = _dual_step(v2, proj, x, Fx_old, data, [1.0], precond)
         g = sigma11 * g1[None] + sigma22 * Ftx                        # sara.m:633
         rel = np.sqrt(rel_x / norm_x) if norm_x > 0 else 0.0
         res, epsn = np.sqrt(gres), np.sqrt(geps)

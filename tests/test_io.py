@@ -87,3 +87,13 @@ def test_channel_data_file_conversion(tmp_path):
     assert d["frequency"] == 1.4e9 and d["max_proj_baseline"] == 1.5e3
     d2 = io.load_channel_data(tmp_path / "ch1.mat", px, apply_imaging_weights=False)
     assert np.allclose(d2["weights"], nW)
+
+
+def test_update_epsilon_rule():
+    """src/update_epsilon.m:52-71: blocks outside [tol_in, tol_out] x eps move
+    towards the residual, at most once per adapt_eps_steps iterations."""
+    from fhs_b200.heuristics import update_epsilon
+    eps, tb = update_epsilon([[10.0, 10.0, 10.0]], 50, [[0, 0, 45]], [[5.0, 20.0, 5.0]], 0.99, 1.001, 10, 0.5)
+    assert eps == [[7.5, 15.0, 10.0]] and tb == [[50, 50, 45]]
+    eps, tb = update_epsilon([[10.0]], 50, [[0]], [[10.0]], 0.99, 1.001, 10, 0.5)
+    assert eps == [[10.0]] and tb == [[0]]

@@ -301,3 +301,29 @@ def test_dr_reduced_data_and_dual_step():
         g2[W] = dr.dr_adjoint(H, lam, v2l)
         assert np.allclose(out[1][l], s22[l] * np.real(data.op.At(g2)))
         assert np.isclose(out[3][l][0], np.linalg.norm(dr.dr_forward(H, lam, Fx[W]) - ddr.y[l][0]))
+
+
+def test_noise_adjustment_rule_and_trigger():
+    """facetHyperSARA.m:883-944: eps_b grows to (eps_b + ||res_b||) c where
+    eps_b < (2 - tol) ||res_b||; FHS adjusts at the run's first iteration,
+    HS at adjust_noise_start_iter; priors stay off until then."""
+    p = so.SolverParams(pdfb_fidelity_tolerance=1.01, adjust_noise_change_percentage=0.5)
+    eps, sig = so.adjust_noise([[1.0, 5.0], [2.0]], [[3.0, 4.0], [1.0]], [[10, 30], [5]], p)
+    assert eps == [[2.0, 5.0], [2.0]]                  # 1 < 0.99*3: raised; 5 >= 0.99*4 and 2 >= 0.99: kept
+    assert np.allclose(sig, [np.sqrt((4 + 25) / 40), np.sqrt(4 / 5)])
+    assert so.adjust_noise_trigger("fhs", 1, 0, 0.0, 10.0, 1.0, p)
+    assert not so.adjust_noise_trigger("hs", 1, 0, 0.0, 10.0, 1.0, p)
+    assert not so.adjust_noise_trigger("fhs", 1, 0, 0.0, 1.0, 1.0, p)   # residual within the bound
+    Ny = Nx = 32
+    data, x, meta = problem.make_problem(Ny, Nx, 2, 800, 2, seed=5, synth=synth)
+    nu2 = so.operator_norm(data, 100, 1e-10)
+    geom = FacetGeometry(Ny, Nx, 2, 2, (4, 4))
+    sig, sig_bar, *_ = so.compute_noise_level(Ny, Nx, 2, np.ones(2), "fhs", geom, nu2)
+    data.eps = [[0.3 * e for e in el] for el in data.eps]
+    kw = dict(nu2=nu2, gamma=sig, gamma0=sig_bar, reweighting_sig=sig, reweighting_sig_bar=sig_bar,
+              pdfb_min_iter=10 ** 6, pdfb_max_iter=8, reweighting_flag=False)
+    xa, loga = so.facet_hypersara(data, so.SolverParams(**kw, adjust_flag_noise=True), geom, max_iter=12)
+    xb, logb = so.facet_hypersara(data, so.SolverParams(**kw), geom, max_iter=12)
+    assert loga.n_adjust >= 1 and loga.epsilon[1] > 10 * loga.epsilon[0]
+    assert all(e1 >= e0 for el0, el1 in zip(data.eps, loga.epsilon_final) for e0, e1 in zip(el0, el1))
+    assert logb.epsilon[-1] == logb.epsilon[0] and not np.allclose(xa, xb)

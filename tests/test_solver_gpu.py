@@ -141,3 +141,24 @@ def test_solver_destroy_after_operator():
     v = np.ones(8, dtype=complex)
     assert np.allclose(proj_l2ball(v, 1.0, 0 * v), v / np.sqrt(8))
     op2.close()
+
+
+@pytest.mark.parametrize("algo", ["fhs", "hs"])
+def test_noise_adjustment_run_matches_oracle(algo):
+    """fhs_solver_run with adjust_flag_noise against the oracle loop: same
+    adjustment iterations, adapted l2 bounds and regularisation parameters,
+    iterates 5e-5 relative after 26 iterations (two adjustments on the way)."""
+    L = 4
+    data, x, op, geom, nu2, sig, sig_bar = _setup(algo, Ny=48, Nx=48, L=L, seed=5, Q=(2, 2), overlap=(5, 5),
+                                                  splits=((0, 22, 48), (0, 25, 48)))
+    data.eps = [[0.3 * e for e in el] for el in data.eps]
+    param = _params(nu2, sig, sig_bar, pdfb_min_iter=10 ** 6, pdfb_max_iter=8, reweighting_flag=False,
+                    adjust_flag_noise=True, adjust_noise_min_iter=5, adjust_noise_start_iter=3)
+    s = _gpu_solver(algo, op, param, geom, data)
+    info = s.run(26)
+    xo, log = _oracle_run(algo, data, param, geom, max_iter=26)
+    assert info["n_iter"] == 26 and info["n_noise_adjustments"] == log.n_adjust >= 2
+    assert rel(np.moveaxis(s.x(), 2, 0), xo) < 5e-5
+    for eg, eo in zip(s.epsilon(), log.epsilon_final):
+        assert np.allclose(eg, eo, rtol=1e-5)
+    s.close()
