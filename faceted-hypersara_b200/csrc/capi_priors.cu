@@ -141,16 +141,15 @@ fhs_status fhs_nuclear_norm(int device, int64_t n_pixels, int L, const double* x
     const int64_t n = n_pixels * L;
     DevBuf<double> st;
     st.alloc(n);
-    DevBuf<float> xf;
-    xf.alloc(n);
     st.upload(x, n, c.s);
-    launch_d2f(st.p, xf.p, n, c.s);
     NucPlan p;
     nuc_plan_init(p, (int)n_pixels, 1, 1, 1, {0, (int)n_pixels}, {0, 1}, 0, 0, FHS_WINDOW_NONE, 1, L, c.s);
     DevBuf<double> val;
     val.alloc(1);
-    nuc_gram(p, xf.p, nullptr, c.s);
-    nuc_eig(p, nullptr, nullptr, val.p, c.s);
+    // FP64 Gram: the small singular values of a nearly low-rank cube need it
+    // (svd() of the reference is FP64)
+    nuc_gram_fp64(p, st.p, n_pixels, c.s);
+    nuc_eig(p, nullptr, nullptr, val.p, c.s, 64.0 * L * 2.220446049250313e-16);
     val.download(f, 1, c.s);
     FHS_CUDA(cudaStreamSynchronize(c.s));
   });

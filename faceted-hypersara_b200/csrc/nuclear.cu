@@ -186,7 +186,8 @@ __device__ __forceinline__ int rr_elem(int i, int r, int m) { return i == 0 ? 0 
 __global__ void __launch_bounds__(256) eig_kernel(const double* __restrict__ gram, int lg,
                                                   const double* __restrict__ weights0,
                                                   const double* __restrict__ beta, float* __restrict__ Mout,
-                                                  double* __restrict__ sigma_out, double* __restrict__ nuc_values) {
+                                                  double* __restrict__ sigma_out, double* __restrict__ nuc_values,
+                                                  double rel_floor) {
   extern __shared__ double sh[];
   const int n = lg;
   double* A = sh;            // n*n
@@ -287,9 +288,11 @@ __global__ void __launch_bounds__(256) eig_kernel(const double* __restrict__ gra
       perm[b] = t;
     }
     double tot = 0.0;
+    // eigenvalues under the Gram's rounding floor are indistinguishable from 0
+    const double floor_lam = rel_floor * fmax(A[perm[0] * n + perm[0]], 0.0);
     for (int i = 0; i < n; ++i) {
       const double lam = A[perm[i] * n + perm[i]];
-      const double sv = sqrt(fmax(lam, 0.0));
+      const double sv = lam > floor_lam ? sqrt(lam) : 0.0;
       sig[i] = sv;
       tot += sv;
       double th = 0.0;
@@ -470,7 +473,92 @@ void nuc_gram(const NucPlan& p, const float* xhat, const float* v0, cudaStream_t
   FHS_LAUNCH_CHECK();
 }
 
-void nuc_eig(const NucPlan& p, const double* weights0, const double* beta, double* nuc_values, cudaStream_t s) {
+// ------------------------------------------------------------ FP64 Gram
+// G = X^T X of an FP64 [L][N] matrix (channel planes), for nuclear_norm:
+// singular values from a Gram eigensolve lose sqrt(Gram error) x sigma_max
+// of absolute accuracy, so a nearly low-rank cube needs the Gram in FP64.
+// CTA = a pixel range staged 64 pixels at a time; thread (bi, bj) owns the
+// 4 x 4 block of channel pairs (4 bi.., 4 bj..), bi <= bj; per-CTA partials
+// are summed in a fixed order (deterministic).
+namespace {
+constexpr int kG64Pix = 64;
+constexpr int kG64PerCta = 16384;
+
+__global__ void __launch_bounds__(256) gram64_partial_kernel(const double* __restrict__ x, int64_t N, int L,
+                                                             double* __restrict__ part) {
+  __shared__ double sx[kG64Pix][kNucMaxL + 1];
+  const int nb = (L + 3) / 4;
+  const int bi = threadIdx.x / 16, bj = threadIdx.x % 16;
+  const bool active = bi < nb && bj < nb && bi <= bj;
+  for (int idx = threadIdx.x; idx < kG64Pix * (kNucMaxL + 1); idx += blockDim.x) (&sx[0][0])[idx] = 0.0;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+  const int64_t p0 = (int64_t)blockIdx.x * kG64PerCta;
+  const int64_t p1 = min(N, p0 + kG64PerCta);
+  for (int64_t base = p0; base < p1; base += kG64Pix) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kG64Pix * L; idx += blockDim.x) {
+      const int l = idx / kG64Pix, q = idx - l * kG64Pix;
+      const int64_t pix = base + q;
+      sx[q][l] = pix < p1 ? x[(int64_t)l * N + pix] : 0.0;
+    }
+    __syncthreads();
+    if (active) {
+      for (int q = 0; q < kG64Pix; ++q) {
+        double a[4], b[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          a[r] = sx[q][4 * bi + r];
+          b[r] = sx[q][4 * bj + r];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+      }
+    }
+  }
+  if (active) {
+    double* o = part + (size_t)blockIdx.x * kNucMaxL * kNucMaxL;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = 4 * bi + r, j = 4 * bj + c;
+        if (i < L && j < L) o[i * kNucMaxL + j] = acc[r][c];
+      }
+  }
+}
+
+__global__ void gram64_reduce_kernel(const double* __restrict__ part, int nparts, int L, double* __restrict__ gram) {
+  const int i = blockIdx.x, j = threadIdx.x;
+  if (j >= L) return;
+  const int a = min(i, j), b = max(i, j);  // partials hold the upper triangle
+  double t = 0.0;
+  for (int k = 0; k < nparts; ++k) t += part[(size_t)k * kNucMaxL * kNucMaxL + a * kNucMaxL + b];
+  gram[i * L + j] = t;
+}
+}  // namespace
+
+void nuc_gram_fp64(const NucPlan& p, const double* x, int64_t N, cudaStream_t s) {
+  FHS_CHECK(p.n_groups == 1 && p.Q == 1, FHS_ERR_INVALID_ARG, "FP64 Gram: one group, one facet");
+  const int nparts = (int)((N + kG64PerCta - 1) / kG64PerCta);
+  DevBuf<double> part;
+  part.alloc((size_t)nparts * kNucMaxL * kNucMaxL);
+  gram64_partial_kernel<<<nparts, 256, 0, s>>>(x, N, p.lg, part.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  gram64_reduce_kernel<<<p.lg, 64, 0, s>>>(part.p, nparts, p.lg, p.gram.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  FHS_CUDA(cudaStreamSynchronize(s));  // part is released on return
+}
+
+void nuc_eig(const NucPlan& p, const double* weights0, const double* beta, double* nuc_values, cudaStream_t s,
+             double rel_floor) {
   const size_t smem = 2 * (size_t)p.lg * p.lg * sizeof(double);
   static bool attr_set[64] = {false};
   int dev = 0;
@@ -480,7 +568,7 @@ void nuc_eig(const NucPlan& p, const double* weights0, const double* beta, doubl
     attr_set[dev] = true;
   }
   eig_kernel<<<p.n_groups * p.Q, 256, smem, s>>>(p.gram.p, p.lg, weights0, beta, p.shrinkM.p, p.sigma.p,
-                                                  nuc_values);
+                                                  nuc_values, rel_floor);
   count_launch();
   FHS_LAUNCH_CHECK();
 }

@@ -37,10 +37,15 @@ void nuc_plan_init(NucPlan& p, int Ny, int Nx, int Qy, int Qx, const std::vector
 
 // Gram_q = Z^T Z with Z = v0_q + D_q .* xhat_q (v0 may be null = 0).
 void nuc_gram(const NucPlan& p, const float* xhat, const float* v0, cudaStream_t s);
+// Gram of one FP64 [lg][N] matrix in FP64 (n_groups = Q = 1 plans), into p.gram.
+void nuc_gram_fp64(const NucPlan& p, const double* x, int64_t N, cudaStream_t s);
 // Jacobi eigensolve of every Gram (FP64), singular values, and the
 // shrinkage matrix for thresholds beta[g*Q+q] * weights0[(g*Q+q)*lg + i].
 // weights0/beta may be null (no thresholding: M = I - I = 0... only sigma used).
-void nuc_eig(const NucPlan& p, const double* weights0, const double* beta, double* nuc_values, cudaStream_t s);
+// rel_floor: eigenvalues <= rel_floor * lambda_max count as 0 (the rounding
+// floor of the Gram; 0 keeps every nonnegative eigenvalue).
+void nuc_eig(const NucPlan& p, const double* weights0, const double* beta, double* nuc_values, cudaStream_t s,
+             double rel_floor = 0.0);
 // v0 <- Z M (rows of Z = pixels).
 void nuc_reconstruct(const NucPlan& p, const float* xhat, float* v0, cudaStream_t s);
 
