@@ -205,11 +205,11 @@ def _traffic_from_profiles(kernel):
     return None
 
 
-def cpu_sample_seconds(seed=0, n_iter=1):
-    """Oracle (FP64 NumPy/SciPy, all host threads) time of one FHS iteration on
-    one channel of one sub-cube at full resolution (1024 x 1024, all of that
-    channel's visibilities, 4x4 facets); the whole-cube estimate scales it by
-    the 64 channels."""
+def _cpu_sample(seed=0):
+    """The oracle's bounded sample of the workload: one channel of one
+    sub-cube at full resolution (1024 x 1024, all of that channel's
+    visibilities, 4x4 facets); returns a function running one FHS iteration
+    (FP64 NumPy/SciPy, all host threads)."""
     import numpy as np
 
     from fhs_b200 import synth
@@ -229,9 +229,17 @@ def cpu_sample_seconds(seed=0, n_iter=1):
     geom = FacetGeometry(Ny, Nx, 4, 4, (26, 26))
     p = so.SolverParams(nu2=np.array([1e3]), gamma=1e-3, gamma0=np.full(16, 1e-2), reweighting_sig=1e-3,
                         reweighting_sig_bar=np.full(16, 1e-2), pdfb_min_iter=10 ** 6, reweighting_flag=False)
-    so.facet_hypersara(data, p, geom, max_iter=1)   # warm-up (allocations, FFT plans)
+    return lambda: so.facet_hypersara(data, p, geom, max_iter=1)
+
+
+def cpu_sample_seconds(seed=0, n_iter=1):
+    """Seconds of one oracle FHS iteration on the sample of _cpu_sample (after
+    one untimed iteration); the whole-cube estimate scales it by 64 channels."""
+    step = _cpu_sample(seed)
+    step()   # warm-up (allocations, FFT plans)
     t0 = time.perf_counter()
-    so.facet_hypersara(data, p, geom, max_iter=n_iter)
+    for _ in range(n_iter):
+        step()
     return (time.perf_counter() - t0) / n_iter
 
 
@@ -248,11 +256,13 @@ def run_reference(args):
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(_ncores()))
     L = WORKLOAD["L"]
+    step = _cpu_sample(0)   # built once; each step is one oracle iteration on it
     times = []
     for i in range(args.warmup + args.steps):
-        t = cpu_sample_seconds(seed=i)
+        t0 = time.perf_counter()
+        step()
         if i >= args.warmup:
-            times.append(t)
+            times.append(time.perf_counter() - t0)
     per_cube = sum(times) / len(times) * L
     value = 1.0 / per_cube
     sample = (f"one FHS iteration of the FP64 oracle on 1 channel (1024x1024, its full visibility set, 4x4 "
