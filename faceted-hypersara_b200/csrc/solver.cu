@@ -860,6 +860,26 @@ fhs_status fhs_solver_epsilon(fhs_solver* s_, double* epsilon) {
   });
 }
 
+fhs_status fhs_solver_set_epsilon(fhs_solver* s_, const double* epsilon) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(epsilon != nullptr, FHS_ERR_INVALID_ARG, "null buffer");
+    FHS_CHECK(S->data_set, FHS_ERR_STATE, "set data first");
+    MeasOp* op = S->op;
+    DeviceGuard dg(op->device);
+    std::vector<double> e((size_t)op->L * kMaxBlocksPerChannel, 0.0);
+    for (int l = 0; l < op->L; ++l)
+      for (int b = 0; b < op->h_nblk[l]; ++b) {
+        const double v = epsilon[op->h_blkoff[l] + b];
+        FHS_CHECK(std::isfinite(v) && v >= 0, FHS_ERR_INVALID_ARG, "epsilon must be finite and >= 0");
+        e[(size_t)l * kMaxBlocksPerChannel + b] = v;
+      }
+    op->blk_eps.upload(e.data(), e.size(), op->stream);
+    S->h_eps.assign(epsilon, epsilon + op->nblk_tot);
+    FHS_CUDA(cudaStreamSynchronize(op->stream));
+  });
+}
+
 fhs_status fhs_solver_regularization(fhs_solver* s_, double* gamma, double* gamma0) {
   return guarded_solver([&] {
     Solver* S = sv(s_);

@@ -116,6 +116,7 @@ SIGNATURES = {
     "fhs_solver_update_weights": (C.c_int, [_vp]),
     "fhs_solver_ellipse_iterations": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "fhs_solver_epsilon": (C.c_int, [_vp, _dp]),
+    "fhs_solver_set_epsilon": (C.c_int, [_vp, _dp]),
     "fhs_solver_regularization": (C.c_int, [_vp, _dp, _dp]),
     "fhs_solver_field_size": (C.c_int64, [_vp, C.c_int]),
     "fhs_solver_get_field": (C.c_int, [_vp, C.c_int, _dp]),

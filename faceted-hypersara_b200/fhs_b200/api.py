@@ -546,9 +546,10 @@ class Solver:
         """The solver state the reference checkpoints (facetHyperSARA.m:1071-1107):
         dict xsol/g [Ny, Nx, L], v0 (flat, per group and facet [P_q, lg]),
         v1 [s, L], v2/proj (nested [l][b] complex), weights0 [lg, Q, groups],
-        weights1 [s, groups]; absent fields are omitted."""
+        weights1 [s, groups], epsilon (nested [l][b], the current l2 bounds);
+        absent fields are omitted."""
         op = self.op
-        out = {}
+        out = {"epsilon": self.epsilon()}
         for name, f in LB.FIELDS.items():
             n = int(lib().fhs_solver_field_size(self._h, f))
             if n <= 0:
@@ -574,6 +575,9 @@ class Solver:
 
     def set_state(self, state):
         """Restores fields of get_state (after init); unknown keys are ignored."""
+        if "epsilon" in state:
+            e = _f64(np.concatenate([np.asarray(b, dtype=np.float64).ravel() for b in state["epsilon"]]))
+            check(lib().fhs_solver_set_epsilon(self._h, dptr(e)))
         for name, f in LB.FIELDS.items():
             if name not in state:
                 continue

@@ -6,7 +6,8 @@
   IEEE big-endian data, 2880-byte records (FITS standard 4.0).
 * ``save_checkpoint`` / ``load_checkpoint`` -- the solver state under the
   field names of the reference's checkpoint files (facetHyperSARA.m:1071-1107:
-  xsol, g, v0, v1, v2, proj, weights0, weights1, plus any scalars given), as a
+  xsol, g, v0, v1, v2, proj, weights0, weights1, epsilon, plus any scalars
+  given), as a
   MATLAB v5 MAT-file (readable by MATLAB's ``load``; scipy writes no v7.3
   HDF5 files, so each variable stays below 2 GB: v1 is a cell of per-channel
   columns).  Layouts are this library's (``Solver.get_state``): x, g, weights
@@ -141,7 +142,7 @@ def save_checkpoint(path, state, **scalars):
     from scipy.io import savemat
     d = {}
     for k, v in state.items():
-        if k in ("v2", "proj"):
+        if k in ("v2", "proj", "epsilon"):
             d[k] = _cells(v)
         elif k == "v1":
             # one [s, L] variable would pass the 2 GB of a v5 variable at large
@@ -169,6 +170,8 @@ def load_checkpoint(path):
             continue
         if k in ("v2", "proj"):
             out[k] = _uncells(v)
+        elif k == "epsilon":
+            out[k] = [[float(b[0]) for b in bl] for bl in _uncells(v)]
         elif k == "v0":
             out[k] = np.asarray(v).ravel(order="F")
         elif k == "v1":

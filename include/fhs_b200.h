@@ -319,6 +319,10 @@ FHS_API fhs_status fhs_solver_ellipse_iterations(fhs_solver* s, int* counts);
 /* Current l2 bounds, one per block (channel-major): the values given to
  * set_data, or as adapted by the noise adjustment of fhs_solver_run. */
 FHS_API fhs_status fhs_solver_epsilon(fhs_solver* s, double* epsilon);
+/* Replaces the l2 bounds (one per block, channel-major) without touching the
+ * data: restores adapted bounds from a checkpoint (the reference saves
+ * epsilon, facetHyperSARA.m:1071-1107). */
+FHS_API fhs_status fhs_solver_set_epsilon(fhs_solver* s, const double* epsilon);
 /* Current regularisation parameters gamma[groups] and gamma0[groups x facets]
  * (gamma0 may be NULL; ignored for SARA). */
 FHS_API fhs_status fhs_solver_regularization(fhs_solver* s, double* gamma, double* gamma0);

@@ -55,3 +55,47 @@ def test_restored_solver_continues_the_run(tmp_path, precond):
     assert rel(b.x(), ref) < 1e-6
     a.close()
     b.close()
+
+
+def test_restore_after_noise_adjustment(tmp_path):
+    """A run whose noise adjustment changed the l2 bounds and the
+    regularisation: the checkpoint carries epsilon, and a solver restored from
+    it (with the adapted gamma / gamma0) continues the original run."""
+    from fhs_b200 import MeasurementOperator, Solver, load_checkpoint, save_checkpoint
+    from fhs_b200._lib import ALGO_FHS
+    Ny = Nx = 48
+    L = 4
+    data, x, meta = problem.make_problem(Ny, Nx, L, Ny * Nx // 2, 2, seed=6, synth=synth)
+    op = MeasurementOperator(Ny, Nx, meta["om"], meta["blocks"],
+                             [np.full(len(o[0]), 1.0 / s) for o, s in zip(meta["om"], meta["sigma"])])
+    nu2 = op.operator_norm(300, 1e-9)
+    geom = FacetGeometry(Ny, Nx, 2, 2, (5, 5))
+    sig, sig_bar, *_ = so.compute_noise_level(Ny, Nx, L, np.ones(L), "fhs", geom, nu2)
+    sig_bar = np.atleast_1d(sig_bar) * np.ones(geom.Q)
+    eps0 = [[0.3 * e for e in el] for el in data.eps]
+    param = dict(nu2=nu2, gamma=sig, gamma0=sig_bar, reweighting_sig=sig, reweighting_sig_bar=sig_bar,
+                 pdfb_min_iter=10 ** 6, pdfb_max_iter=8, reweighting_flag=False, adjust_flag_noise=True)
+    kw = dict(Qy=2, Qx=2, overlap=(5, 5), splits_y=[r[0] for r in geom.base_y] + [Ny],
+              splits_x=[r[0] for r in geom.base_x] + [Nx])
+    a = Solver(op, ALGO_FHS, param, **kw)
+    a.set_data(data.y, eps0)
+    a.init()
+    info = a.run(6)
+    assert info["n_noise_adjustments"] >= 1
+    state = a.get_state()
+    assert not np.allclose(state["epsilon"][0], eps0[0])
+    path = tmp_path / "ckpt.mat"
+    save_checkpoint(path, state, end_iter=6)
+    g, g0 = a.regularization()
+    a.iterate(4)
+    ref = a.x()
+    b = Solver(op, ALGO_FHS, dict(param, gamma=g, gamma0=g0, adjust_flag_noise=False), **kw)
+    b.set_data(data.y, eps0)
+    restored = load_checkpoint(path)
+    b.init(restored["xsol"])
+    b.set_state(restored)
+    assert np.allclose(np.concatenate(b.epsilon()), np.concatenate(state["epsilon"]), rtol=0, atol=0)
+    b.iterate(4)
+    assert rel(b.x(), ref) < 1e-6
+    a.close()
+    b.close()

@@ -52,6 +52,7 @@ def test_checkpoint_round_trip(tmp_path):
                for _ in range(4)],
         "weights0": rng.random((4, 2, 2)),
         "weights1": rng.random((30, 2)),
+        "epsilon": [[1.5, 2.25] for _ in range(4)],
     }
     p = tmp_path / "ckpt.mat"
     io.save_checkpoint(p, state, end_iter=17, rel_val=np.array([0.1, 0.01]))
@@ -62,6 +63,7 @@ def test_checkpoint_round_trip(tmp_path):
     for l in range(4):
         for b in range(2):
             assert np.array_equal(back["v2"][l][b], state["v2"][l][b])
+    assert back["epsilon"] == state["epsilon"]
     assert int(back["end_iter"].ravel()[0]) == 17
 
 
