@@ -1,4 +1,5 @@
-"""Build ``fhs_b200/libfhs_b200.so`` for sm_100a with nvcc (in-tree).
+"""Build ``fhs_b200/libfhs_b200.so`` for sm_100a with nvcc (in-tree), and the
+standalone C harness ``fhs_b200/fhs_harness`` over its C ABI (gcc).
 
 Usage: ``python faceted-hypersara_b200/build.py [--force]``.  Objects go to
 ``faceted-hypersara_b200/_build/`` (git-ignored); the shared library is
@@ -16,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "fhs_b200", "libfhs_b200.so")
+HARNESS = os.path.join(HERE, "fhs_b200", "fhs_harness")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -70,6 +72,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if jobs or force or not os.path.exists(OUT):
         cmd = [nvcc, *ARCH, "-shared", "-o", OUT, *objs, "-lcufft", "-lcudart"]
         run(cmd)
+    # the standalone C harness (plain C99 over the C ABI), next to the library
+    hsrc = os.path.join(HERE, "harness", "fhs_harness.c")
+    if force or not os.path.exists(HARNESS) or os.path.getmtime(HARNESS) < max(
+            os.path.getmtime(hsrc), os.path.getmtime(OUT), hdr_mtime):
+        cc = shutil.which("gcc") or shutil.which("cc")
+        if cc is None:
+            raise RuntimeError("no C compiler for the harness")
+        run([cc, "-O2", "-std=c99", "-D_POSIX_C_SOURCE=200809L", "-Wall", "-I", INCLUDE, hsrc,
+             "-L", os.path.dirname(OUT), "-lfhs_b200", "-Wl,-rpath,$ORIGIN", "-lm", "-o", HARNESS])
     return OUT
 
 

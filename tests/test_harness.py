@@ -1,0 +1,67 @@
+"""The standalone C harness (faceted-hypersara_b200/harness/fhs_harness.c):
+a plain C99 program over the C ABI, configured by a JSON file in the layout
+of the reference's imaging/default_parameters.json plus a "harness" section.
+
+CPU: configuration parsing (--dry-run touches no GPU) and error exits.
+GPU: small FHS / HS / SARA problems, preconditioned and visibility-gridding
+variants, solved to the reference's stopping rule; the reconstruction SNR
+against the synthetic ground truth stands in for correctness (the solver
+arithmetic itself is checked against the oracle by the other GPU tests).
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HARNESS = os.path.join(ROOT, "faceted-hypersara_b200", "fhs_b200", "fhs_harness")
+CONFIG = os.path.join(ROOT, "faceted-hypersara_b200", "harness", "example_config.json")
+
+needs_harness = pytest.mark.skipif(not os.path.exists(HARNESS), reason="harness not built (run build())")
+
+
+def _run(*args, timeout=600):
+    r = subprocess.run([HARNESS, *args], capture_output=True, text=True, timeout=timeout)
+    return r.returncode, r.stdout, r.stderr
+
+
+@needs_harness
+def test_dry_run_reads_the_reference_layout():
+    rc, out, err = _run(CONFIG, "--dry-run")
+    assert rc == 0, err
+    d = json.loads(out)
+    assert d["algo"] == "fhs" and (d["Ny"], d["Nx"], d["L"]) == (128, 128, 8)
+    assert (d["oy"], d["J"], d["nlevel"]) == (2, 7, 4)
+    assert d["pdfb_max_iter"] == 150 and d["reweighting_max_iter"] == 1 and d["elipse_proj_max_iter"] == 20
+    rc, out, err = _run(CONFIG, "algo=sara", "Ny=64", "dr=1", "--dry-run")
+    d = json.loads(out)
+    assert rc == 0 and d["algo"] == "sara" and d["L"] == 1 and d["Qy"] == 1 and d["Ny"] == 64 and d["dr"] == 1
+
+
+@needs_harness
+def test_configuration_errors_exit_1(tmp_path):
+    bad = tmp_path / "bad.json"
+    bad.write_text('[{"pdfb": {"max_iter": }]')
+    assert _run(str(bad), "--dry-run")[0] == 1
+    assert _run(str(tmp_path / "missing.json"), "--dry-run")[0] == 1
+    assert _run(CONFIG, "n_blocks=17", "--dry-run")[0] == 1
+    assert _run(CONFIG, "precond=1", "dr=1", "--dry-run")[0] == 1
+
+
+@pytest.mark.gpu
+@needs_harness
+@pytest.mark.parametrize("args,min_snr", [
+    (("Ny=64", "Nx=64", "L=4"), 18.0),
+    (("algo=hs", "Ny=64", "Nx=64", "L=4"), 18.0),
+    (("algo=sara", "Ny=64", "Nx=64"), 20.0),
+    (("Ny=64", "Nx=64", "L=4", "precond=1"), 18.0),
+    (("Ny=64", "Nx=64", "L=4", "dr=1", "vis_fraction=2"), 18.0),
+])
+def test_harness_solves(tmp_path, args, min_snr):
+    out = tmp_path / "x.bin"
+    rc, so, err = _run(CONFIG, *args, f"output={out}")
+    assert rc == 0, err
+    d = json.loads(so.strip().splitlines()[-1])
+    assert d["n_iter"] >= 1 and d["snr_db"] > min_snr, d
+    assert out.stat().st_size == 8 * d["Ny"] * d["Nx"] * d["L"]
