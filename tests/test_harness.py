@@ -65,3 +65,17 @@ def test_harness_solves(tmp_path, args, min_snr):
     d = json.loads(so.strip().splitlines()[-1])
     assert d["n_iter"] >= 1 and d["snr_db"] > min_snr, d
     assert out.stat().st_size == 8 * d["Ny"] * d["Nx"] * d["L"]
+
+
+def test_mex_gateway_compiles_against_the_abi():
+    """faceted-hypersara_b200/mex/fhs_mex.c type-checks against include/fhs_b200.h
+    (MATLAB's mex.h is absent here: tests/mex_stub/mex.h declares the calls it uses)."""
+    import shutil
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    r = subprocess.run([cc, "-fsyntax-only", "-std=c99", "-Wall", "-Wextra", "-Werror",
+                        "-I", os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "tests", "mex_stub"),
+                        os.path.join(ROOT, "faceted-hypersara_b200", "mex", "fhs_mex.c")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
