@@ -349,7 +349,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                 "algorithmic_bytes": nbytes[dom], "ms_per_launch": mine[dom],
-                "traffic": _traffic_from_profiles(("dr_" if args.dr else "") + dom)}
+                "traffic": _traffic_from_profiles("dr_apply" if args.dr else dom)}
     stage_rows = {k: {"ms": round(v, 4), **({"gbs": round(nbytes[k] / (v / 1e3) / 1e9, 1)} if k in nbytes and v > 0
                                            else {})} for k, v in stages.items()}
     # ---- end to end through the public API with pinned host buffers

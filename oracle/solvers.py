@@ -6,7 +6,8 @@ Arrays are channel-first here: an image cube is ``x[L, Ny, Nx]``.  Each
 function cites the reference file it restates.  The data-fidelity dual takes
 either the l2-ball form (``pU = 1``, ``update_dual_data_fidelity.m:83``) or,
 with a ``Precond``, the preconditioned ellipsoid projection
-(``update_dual_data_fidelity.m:126-147``).  Visibility gridding (DR) is off.
+(``update_dual_data_fidelity.m:126-147``).  Visibility gridding (DR) runs
+through the same routines on the DR data term of ``oracle/dr.py``.
 
 The ellipsoid projection ``solver_proj_elipse_fb`` and the uniform-weight
 preconditioner ``util_gen_preconditioning_matrix`` belong to the
