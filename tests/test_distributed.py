@@ -44,3 +44,25 @@ def test_max_over_ranks_and_weak_scaling_value():
         assert p.exitcode == 0
     assert [o[1] for o in out] == [150.0, 150.0]
     assert out[0][2] == pytest.approx(2 * 20 / 0.150)
+
+
+def test_algorithmic_bytes_per_launch():
+    """bench.py's roofline numerators: the per-launch byte formulas of the
+    visibility (l2-ball and preconditioned) and DR data terms."""
+    from types import SimpleNamespace
+
+    import bench
+    L, Ny, Nx, M = 4, 64, 64, 10000
+    No = 4 * Ny * Nx
+    op = SimpleNamespace(L=L, Ny=Ny, Nx=Nx, No=No, n_vis_total=3000, block_sizes=[[M // L]] * L)
+    prob = dict(op=op, n_vis=M, Q=2, splits=([0, 32, 64], [0, 32, 64]), overlap=(4, 4), C=1)
+    b = bench.algorithmic_bytes(prob, 9 * Ny * Nx)
+    assert b["degrid_dual"] == No * L * 8 + M * 56
+    assert b["grid_dual"] == M * 32 + No * L * 8
+    bp = bench.algorithmic_bytes(dict(prob, precond=True), 9 * Ny * Nx, [[2] for _ in range(L)])
+    assert bp["degrid_dual"] == b["degrid_dual"] + 20 * M and bp["ellipse_fb"] == 2 * M * 53
+    bd = bench.algorithmic_bytes(dict(prob, dr=True), 9 * Ny * Nx)
+    n = op.n_vis_total
+    stencil = n * (85 * 8 + 8) + L * No * 4
+    assert bd["degrid_dual"] == stencil + L * (No // 2) * 8 + n * 40
+    assert bd["grid_dual"] == stencil + n * 16 + L * No * 8
