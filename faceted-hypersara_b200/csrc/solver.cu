@@ -93,41 +93,66 @@ struct AssembleArgs {
   int64_t v0_group;
 };
 
-__global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, float* __restrict__ g,
+// g = sigma22 s Re(At(...)) + sigma11 Psi v1 (in g1) + sigma00 sum_q D_q v0_q.
+// One thread per pixel walks every channel plane: the pixel's facets (up to
+// four overlapping ones), their window values and dual offsets are looked up
+// once and reused by all L planes; each plane's accesses stay coalesced
+// across the warp (consecutive pixels of a column).
+__global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, int L, float* __restrict__ g,
                                                        const float* __restrict__ img, const float* __restrict__ g1,
                                                        const float* __restrict__ v0, const float* __restrict__ sigma22,
                                                        const float* __restrict__ sy, const float* __restrict__ sx) {
-  const int plane = blockIdx.y;
-  const int grp = plane / a.lg, lc = plane - grp * a.lg;
   const int64_t N = (int64_t)a.Ny * a.Nx;
-  const float s22 = sigma22[plane];
-  const float* gp = img + (size_t)plane * a.Ky * a.Kx;  // Re(IFFT(gridB)), [Kx][Ky]
+  const int64_t plane_img = (int64_t)a.Ky * a.Kx;  // Re(IFFT(gridB)) planes, [Kx][Ky]
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
     const int ix = (int)(p / a.Ny), iy = (int)(p - (int64_t)ix * a.Ny);
     int ky = iy - a.Ny / 2;
     ky += ky < 0 ? a.Ky : 0;
     int kx = ix - a.Nx / 2;
     kx += kx < 0 ? a.Kx : 0;
-    float val = s22 * sy[iy] * sx[ix] * gp[(size_t)kx * a.Ky + ky] + g1[(size_t)plane * N + p];
+    const int64_t kimg = (int64_t)kx * a.Ky + ky;
+    const float syi = sy[iy], sxi = sx[ix];
+    int ne = 0;
+    int64_t base[4], P[4];
+    float w[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      base[e] = 0;
+      P[e] = 0;
+      w[e] = 0.f;
+    }
     if (a.nuclear) {
-      float acc = 0.f;
+#pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int qy = a.cover_y[2 * iy + i];
-        if (qy < 0) continue;
+#pragma unroll
         for (int j = 0; j < 2; ++j) {
           const int qx = a.cover_x[2 * ix + j];
-          if (qx < 0) continue;
+          if (qy < 0 || qx < 0) continue;
           const NucFacet f = a.facets[qx * a.Qy + qy];
           const int ny = f.y1 - f.y0;
           const int ly = iy - f.y0, lx = ix - f.x0;
-          const int64_t P = (int64_t)ny * (f.x1 - f.x0);
-          const float w = a.wy[f.wy_off + ly] * a.wx[f.wx_off + lx];
-          acc = fmaf(w, v0[(int64_t)grp * a.v0_group + f.v0_off + (int64_t)lc * P + (int64_t)lx * ny + ly], acc);
+          const int slot = 2 * i + j;
+          base[slot] = f.v0_off + (int64_t)lx * ny + ly;
+          P[slot] = (int64_t)ny * (f.x1 - f.x0);
+          w[slot] = a.wy[f.wy_off + ly] * a.wx[f.wx_off + lx];
+          ne |= 1 << slot;
         }
       }
-      val = fmaf(a.sigma00, acc, val);
     }
-    g[(size_t)plane * N + p] = val;
+    for (int plane = 0; plane < L; ++plane) {
+      const int grp = plane / a.lg, lc = plane - grp * a.lg;
+      float val = sigma22[plane] * syi * sxi * img[(size_t)plane * plane_img + kimg] + g1[(size_t)plane * N + p];
+      if (ne) {
+        float acc = 0.f;
+        const float* vg = v0 + (int64_t)grp * a.v0_group;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (ne & (1 << e)) acc = fmaf(w[e], vg[base[e] + (int64_t)lc * P[e]], acc);
+        val = fmaf(a.sigma00, acc, val);
+      }
+      g[(size_t)plane * N + p] = val;
+    }
   }
 }
 
@@ -300,8 +325,8 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   a.cover_y = S->nuclear ? S->np.cover_y.p : nullptr;
   a.cover_x = S->nuclear ? S->np.cover_x.p : nullptr;
   a.v0_group = S->nuclear ? S->np.v0_group : 0;
-  assemble_kernel<<<dim3(nblk(S->N), L), 256, 0, s>>>(a, S->g.p, op->imgr.p, S->g1.p, S->v0.p, S->sigma22.p,
-                                                     op->sy.p, op->sx.p);
+  assemble_kernel<<<nblk(S->N), 256, 0, s>>>(a, L, S->g.p, op->imgr.p, S->g1.p, S->v0.p, S->sigma22.p,
+                                           op->sy.p, op->sx.p);
   count_launch();
   FHS_LAUNCH_CHECK();
   mark();
