@@ -60,20 +60,32 @@ __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, 
   float* hp = xhat + (size_t)plane * N;
   float* pp = pad + (size_t)plane * Ky * Kx;
   double a = 0.0, b = 0.0;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x) {
-    const float xo = xp[p];
-    const float xn = fmaxf(xo - gp[p], 0.f);
-    xp[p] = xn;
-    hp[p] = 2.f * xn - xo;
-    const double d = (double)xo - xn;
-    a += d * d;
-    b += (double)xn * xn;
-    const int ix = (int)(p / Ny), iy = (int)(p - (int64_t)ix * Ny);
-    int ky = iy - Ny / 2;
-    ky += ky < 0 ? Ky : 0;
-    int kx = ix - Nx / 2;
-    kx += kx < 0 ? Kx : 0;
-    pp[(size_t)kx * Ky + ky] = xn * sy[iy] * sx[ix];
+  // four pixels per step (N is a multiple of 4: Ny and Nx are even), float4
+  // loads and stores of x, g and xhat for memory-level parallelism
+  const int64_t N4 = N / 4;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N4; q += (int64_t)gridDim.x * blockDim.x) {
+    const float4 xo4 = reinterpret_cast<const float4*>(xp)[q];
+    const float4 g4 = reinterpret_cast<const float4*>(gp)[q];
+    const float xo[4] = {xo4.x, xo4.y, xo4.z, xo4.w};
+    const float gv[4] = {g4.x, g4.y, g4.z, g4.w};
+    float xn[4], xh[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      xn[e] = fmaxf(xo[e] - gv[e], 0.f);
+      xh[e] = 2.f * xn[e] - xo[e];
+      const double d = (double)xo[e] - xn[e];
+      a += d * d;
+      b += (double)xn[e] * xn[e];
+      const int64_t p = 4 * q + e;
+      const int ix = (int)(p / Ny), iy = (int)(p - (int64_t)ix * Ny);
+      int ky = iy - Ny / 2;
+      ky += ky < 0 ? Ky : 0;
+      int kx = ix - Nx / 2;
+      kx += kx < 0 ? Kx : 0;
+      pp[(size_t)kx * Ky + ky] = xn[e] * sy[iy] * sx[ix];
+    }
+    reinterpret_cast<float4*>(xp)[q] = make_float4(xn[0], xn[1], xn[2], xn[3]);
+    reinterpret_cast<float4*>(hp)[q] = make_float4(xh[0], xh[1], xh[2], xh[3]);
   }
   block_sum2(a, b);
   if (threadIdx.x == 0) {
