@@ -79,3 +79,17 @@ def test_mex_gateway_compiles_against_the_abi():
                         os.path.join(ROOT, "faceted-hypersara_b200", "mex", "fhs_mex.c")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@needs_harness
+def test_dry_run_accepts_a_single_object(tmp_path):
+    """A configuration may also be one JSON object holding the sections."""
+    cfg = tmp_path / "one.json"
+    cfg.write_text(json.dumps({"pdfb": {"max_iter": 77}, "sara": {"nlevel": 3},
+                               "aux_global": {"measop_flag_visibility_gridding": True},
+                               "harness": {"algo": "hs", "Ny": 96, "Nx": 80, "L": 5, "snr_db": 30}}))
+    rc, out, err = _run(str(cfg), "--dry-run")
+    assert rc == 0, err
+    d = json.loads(out)
+    assert (d["algo"], d["Ny"], d["Nx"], d["L"], d["Qy"]) == ("hs", 96, 80, 5, 1)
+    assert d["pdfb_max_iter"] == 77 and d["nlevel"] == 3 and d["dr"] == 1 and d["snr_db"] == 30
