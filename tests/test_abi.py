@@ -63,3 +63,25 @@ def test_package_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
     with pytest.raises(ImportError):
         _lib.lib()
+
+
+def test_null_handles_of_the_dr_and_solver_accessors():
+    """The entry points added for visibility gridding and the noise adjustment
+    reject null handles and buffers with a status, without touching a GPU."""
+    import ctypes as C
+
+    import numpy as np
+    from fhs_b200 import _lib
+    L = _lib.lib()
+    out = C.c_void_p()
+    buf = np.zeros(4)
+    cells = np.zeros(4, dtype=np.int64)
+    assert L.fhs_measop_create_dr(None, C.byref(out)) == 1 and not out.value
+    assert L.fhs_measop_create_dr(None, None) == 1
+    assert L.fhs_measop_is_dr(None) == -1
+    assert L.fhs_measop_dr_cells(None, 0, cells.ctypes.data_as(C.POINTER(C.c_int64))) == 1
+    assert L.fhs_measop_dr_lambda(None, 0, _lib.dptr(buf)) == 1
+    for fn in (L.fhs_solver_epsilon, L.fhs_solver_set_epsilon):
+        assert fn(None, _lib.dptr(buf)) != 0
+    assert L.fhs_solver_regularization(None, _lib.dptr(buf), None) != 0
+    assert L.fhs_last_error() != b""
