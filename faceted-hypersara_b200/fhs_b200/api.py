@@ -11,11 +11,14 @@ Function names, argument meaning and return values follow the reference
   ``gen_preconditioning_matrix``                          (lib/operators/, util_gen_preconditioning_matrix)
 * ``proj_l2ball``, ``nuclear_norm``, ``compute_sara_prior`` (src/*.m:1)
 * ``facetHyperSARA``, ``hyperSARA``, ``sara``              (src/{fhs,hs,sara}/*.m:1)
+* ``MeasurementOperator.dimensionality_reduction`` / ``reduce_data``
+                    (lib/operators/util_load_data_gen_dr_measurement_operator.m)
 
 Image cubes are ``[Ny, Nx, L]`` float64 arrays (MATLAB order is used on the
 wire: Fortran-contiguous copies are made as needed).  Visibilities and l2
 bounds are nested lists ``y[l][b]`` / ``epsilon[l][b]`` as the reference's
-cells.  The operator handle replaces the reference's ``A, At, G, W`` tuple.
+cells.  The operator handle replaces the reference's ``A, At, G, W`` tuple
+(and ``Lambda`` for a visibility-gridding operator).
 Every computation runs in ``libfhs_b200.so`` on the GPU; a missing library or
 device raises.
 """
@@ -266,8 +269,8 @@ def gen_preconditioning_matrix(om_y, om_x, Ky, Kx, sub_pixels=1):
 
 
 def compute_residual_images(x, y, op: MeasurementOperator):
-    """src/compute_residual_images.m:83-102 (no DR): PSF-normalised residual
-    images real(At(G'(y - G A x))) -> [Ny, Nx, L]."""
+    """src/compute_residual_images.m:83-102 (DR operator: :42-80): PSF-normalised
+    residual images real(At(G'(y - G A x))) -> [Ny, Nx, L]."""
     xc = _cube_in(x, op.Ny, op.Nx)
     yf = _cplx_in(np.concatenate([op.flatten(v) for v in y]))
     out = np.empty(op.Ny * op.Nx * op.L)
@@ -341,7 +344,8 @@ def compute_sara_prior(x, nlevel=4, device: int = 0):
 
 
 def update_dual_data_fidelity(v2, y, x, Fx_old, op: MeasurementOperator, epsilon, sigma22):
-    """src/update_dual_data_fidelity.m:1-6 with pU = 1 and no DR.
+    """src/update_dual_data_fidelity.m:1-6 with pU = 1 (a DR operator takes the
+    flag_dimensionality_reduction branch, :85-125).
 
     Returns (v2, Ftx, Fx_old, norm_res, global_norm_res, norm_epsilon) with the
     reference's meaning (v2/norm_res as nested lists, Fx_old [No, L])."""
@@ -640,7 +644,8 @@ def facetHyperSARA(y, epsilon, op: MeasurementOperator, param: dict, Qx, Qy, nle
                    splits_x=None, max_iter=0):
     """src/fhs/facetHyperSARA.m:1-6 -> (xsol [Ny, Nx, L], info).  The
     reference's A, At, G, W are the operator handle and pU its preconditioner
-    (none: pU = 1); no DR."""
+    (none: pU = 1); a DR operator (MeasurementOperator.dimensionality_reduction)
+    runs the reference's flag_dimensionality_reduction path."""
     s = Solver(op, LB.ALGO_FHS, param, nlevel, n_groups, Qy, Qx, overlap_size, window_type, splits_y, splits_x)
     try:
         s.set_data(y, epsilon)
