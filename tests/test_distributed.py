@@ -66,3 +66,19 @@ def test_algorithmic_bytes_per_launch():
     stencil = n * (85 * 8 + 8) + L * No * 4
     assert bd["degrid_dual"] == stencil + L * (No // 2) * 8 + n * 40
     assert bd["grid_dual"] == stencil + n * 16 + L * No * 8
+
+
+def test_reference_arm_prints_the_contract_line():
+    """bench.py --impl reference (the FP64 oracle on the host cores) prints one
+    JSON line with the keys the bench contract asks of the reference arm."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=900, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "iter/s" and d["steps"] == 1
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
