@@ -147,3 +147,42 @@ def test_large_spectral_groups(L):
     xo, _ = so.facet_hypersara(data, so.SolverParams(**param), geom, max_iter=5)
     assert rel(np.moveaxis(s.x(), 2, 0), xo) < ITER_TOL
     s.close()
+
+
+def test_single_visibility_blocks():
+    """Blocks holding one visibility and a channel with one visibility in all:
+    operators and the l2-ball dual step against the oracle.  A single
+    visibility's G Fx is a sum of 49 FP32 products that can cancel, so its
+    error is measured against the operand scale ||(|G| |Fx|)_b|| (block
+    residual norms within 2e-5 of it; the other blocks' observed errors are
+    below 2e-6 of it), and v2 is drawn at 10x that scale so that z = v2 +
+    2 G Fx - G Fx_old - y does not cancel."""
+    from fhs_b200 import HS_adjoint_operator_G, HS_forward_operator_G, MeasurementOperator, \
+        update_dual_data_fidelity
+    Ny, Nx = 32, 24
+    oy0, ox0 = coverage(1000, 12)
+    om = [(oy0, ox0), (oy0[:1], ox0[:1]), (oy0[:3], ox0[:3])]
+    sizes = [[1, 1, 998], [1], [1, 1, 1]]
+    data, x = _data(Ny, Nx, om, sizes, 9)
+    op = MeasurementOperator(Ny, Nx, om, sizes)
+    yg = HS_forward_operator_G(np.moveaxis(x, 0, 2), op)
+    yo = so.forward_operator(x, data)
+    for l in range(3):
+        assert rel(np.concatenate(yg[l]), np.concatenate(yo[l])) < OP_TOL
+    rng = np.random.default_rng(4)
+    v = [[rng.standard_normal(len(b)) + 1j * rng.standard_normal(len(b)) for b in yl] for yl in data.y]
+    assert rel(np.moveaxis(HS_adjoint_operator_G(v, op), 2, 0), so.adjoint_operator(v, data)) < OP_TOL
+    # FP32 operand scale of G Fx per block, at the dual step's x
+    scale = [[float(np.linalg.norm(abs(G) @ abs(data.op.A(0.9 * x[l])))) for G in data.G[l]] for l in range(3)]
+    v2 = [[10.0 * np.sqrt(sum(t * t for t in sl) / sum(map(len, yl))) * b for b in vl]
+          for yl, vl, sl in zip(data.y, v, scale)]
+    Fx_old = np.stack([data.op.A(x[l] * 0.8) for l in range(3)])
+    s22 = np.array([0.5, 0.3, 0.2])
+    ref = so.update_dual_data_fidelity(v2, x * 0.9, Fx_old, data, s22)
+    v2g, Ftx, Fx_new, norm_res, gres, geps = update_dual_data_fidelity(
+        v2, data.y, np.moveaxis(x * 0.9, 0, 2), Fx_old.T, op, data.eps, s22)
+    for l in range(3):
+        assert rel(np.concatenate(v2g[l]), np.concatenate(ref[0][l])) < OP_TOL
+        for b in range(len(sizes[l])):
+            assert abs(norm_res[l][b] - ref[3][l][b]) <= 2e-5 * scale[l][b], (l, b)
+    assert rel(np.moveaxis(Ftx, 2, 0), ref[1]) < 1e-4
