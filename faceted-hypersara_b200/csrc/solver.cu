@@ -777,7 +777,7 @@ static void adjust_noise_level(Solver* S) {
     double ssum = 0.0;
     for (int i = 0; i < lg; ++i) {
       const int l = g * lg + i;
-      ssum += sig_ch[l] * sig_ch[l] / S->nu2[l];
+      if (S->nu2[l] > 0) ssum += sig_ch[l] * sig_ch[l] / S->nu2[l];  // a channel without data adds nothing
     }
     const double sig_sara = std::sqrt(ssum / lg);
     S->gamma[g] = S->alph * sig_sara * (mu_chi + sig_chi);

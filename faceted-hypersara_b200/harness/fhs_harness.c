@@ -445,6 +445,11 @@ int main(int argc, char** argv) {
   int rc = 0;
   const int Ny = pc.Ny, Nx = pc.Nx, L = pc.L, Q = pc.Qy * pc.Qx;
   const int64_t N = (int64_t)Ny * Nx, M = (int64_t)(pc.vis_fraction * N);
+  if (M < (int64_t)pc.n_blocks) {
+    fprintf(stderr, "fhs_harness: vis_fraction gives fewer visibilities than blocks\n");
+    jfree(root);
+    return 1;
+  }
   g_rng = 0x5EEDULL + (uint64_t)pc.seed;
   double *x_true = NULL, *om_y = NULL, *om_x = NULL, *y = NULL, *y0 = NULL, *eps = NULL, *sig = NULL,
          *nu2 = NULL, *xs = NULL, *pu = NULL, *gridv = NULL, *lam = NULL, *noise = NULL;

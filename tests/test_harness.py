@@ -47,6 +47,7 @@ def test_configuration_errors_exit_1(tmp_path):
     assert _run(str(tmp_path / "missing.json"), "--dry-run")[0] == 1
     assert _run(CONFIG, "n_blocks=17", "--dry-run")[0] == 1
     assert _run(CONFIG, "precond=1", "dr=1", "--dry-run")[0] == 1
+    assert _run(CONFIG, "vis_fraction=1e-9")[0] == 1   # rejected before any GPU call
 
 
 @pytest.mark.gpu
