@@ -86,7 +86,6 @@ static int64_t total_vis(fhs_measop* op, int L) {
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   char cmd[64];
   need(nrhs >= 1 && mxIsChar(prhs[0]) && mxGetString(prhs[0], cmd, sizeof cmd) == 0, "first input: command");
-  (void)nlhs;
   if (!strcmp(cmd, "measop_create")) {
     need(nrhs == 8, "measop_create(Ny, Nx, oy, ox, J, L, device)");
     fhs_measop* op = NULL;
@@ -151,16 +150,27 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     need(nrhs == 8, "update_dual_data_fidelity(h, v2, y, x, Fx_old, epsilon, sigma22)");
     fhs_measop* op = op_of(prhs[1]);
     const mwSize* d = mxGetDimensions(prhs[4]);
-    plhs[0] = mxDuplicateArray(prhs[2]);                                   /* v2 (updated) */
-    plhs[1] = mxCreateNumericArray(mxGetNumberOfDimensions(prhs[4]), d, mxDOUBLE_CLASS, mxREAL);  /* Ftx */
-    plhs[2] = mxDuplicateArray(prhs[5]);                                   /* Fx_old (updated) */
-    plhs[3] = mxCreateDoubleMatrix(mxGetNumberOfElements(prhs[6]), 1, mxREAL); /* norm_res per block */
-    plhs[4] = mxCreateDoubleScalar(0.0);
-    plhs[5] = mxCreateDoubleScalar(0.0);
-    check(fhs_update_dual_data_fidelity(op, (double*)mxGetComplexDoubles(plhs[0]), cplx_in(prhs[3]),
-                                        real_in(prhs[4]), (double*)mxGetComplexDoubles(plhs[2]),
-                                        real_in(prhs[6]), real_in(prhs[7]), mxGetDoubles(plhs[1]),
-                                        mxGetDoubles(plhs[3]), mxGetDoubles(plhs[4]), mxGetDoubles(plhs[5])));
+    (void)cplx_in(prhs[2]);  /* v2 and Fx_old must be complex (usage error otherwise) */
+    (void)cplx_in(prhs[5]);
+    mxArray* out[6];
+    out[0] = mxDuplicateArray(prhs[2]);                                    /* v2 (updated) */
+    out[1] = mxCreateNumericArray(mxGetNumberOfDimensions(prhs[4]), d, mxDOUBLE_CLASS, mxREAL);  /* Ftx */
+    out[2] = mxDuplicateArray(prhs[5]);                                    /* Fx_old (updated) */
+    out[3] = mxCreateDoubleMatrix(mxGetNumberOfElements(prhs[6]), 1, mxREAL); /* norm_res per block */
+    out[4] = mxCreateDoubleScalar(0.0);
+    out[5] = mxCreateDoubleScalar(0.0);
+    const fhs_status st = fhs_update_dual_data_fidelity(
+        op, (double*)mxGetComplexDoubles(out[0]), cplx_in(prhs[3]), real_in(prhs[4]),
+        (double*)mxGetComplexDoubles(out[2]), real_in(prhs[6]), real_in(prhs[7]), mxGetDoubles(out[1]),
+        mxGetDoubles(out[3]), mxGetDoubles(out[4]), mxGetDoubles(out[5]));
+    /* plhs holds max(nlhs, 1) entries: hand over the requested outputs only */
+    for (int k = 0; k < 6; ++k) {
+      if (k < nlhs || k == 0)
+        plhs[k] = out[k];
+      else
+        mxDestroyArray(out[k]);
+    }
+    check(st);
   } else if (!strcmp(cmd, "proj_l2ball")) { /* src/proj_l2ball.m:1 */
     const mwSize n = mxGetNumberOfElements(prhs[1]);
     plhs[0] = mxCreateDoubleMatrix(n, 1, mxCOMPLEX);
@@ -242,14 +252,16 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     if (st == FHS_OK) st = fhs_solver_get_x(s, mxGetDoubles(plhs[0]));
     fhs_solver_destroy(s);
     check(st);
-    plhs[1] = mxCreateDoubleMatrix(1, 6, mxREAL);
-    double* o = mxGetDoubles(plhs[1]);
-    o[0] = ri.n_iter;
-    o[1] = ri.n_reweights;
-    o[2] = ri.converged;
-    o[3] = ri.rel_val;
-    o[4] = ri.residual;
-    o[5] = ri.seconds;
+    if (nlhs > 1) { /* info = [n_iter, n_reweights, converged, rel_val, residual, seconds] */
+      plhs[1] = mxCreateDoubleMatrix(1, 6, mxREAL);
+      double* o = mxGetDoubles(plhs[1]);
+      o[0] = ri.n_iter;
+      o[1] = ri.n_reweights;
+      o[2] = ri.converged;
+      o[3] = ri.rel_val;
+      o[4] = ri.residual;
+      o[5] = ri.seconds;
+    }
   } else {
     mexErrMsgIdAndTxt("fhs:usage", "unknown command '%s'", cmd);
   }

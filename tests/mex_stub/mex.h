@@ -42,4 +42,5 @@ mxArray* mxCreateDoubleScalar(double v);
 mxArray* mxCreateNumericMatrix(mwSize m, mwSize n, mxClassID id, mxComplexity c);
 mxArray* mxCreateNumericArray(mwSize ndim, const mwSize* dims, mxClassID id, mxComplexity c);
 mxArray* mxDuplicateArray(const mxArray* a);
+void mxDestroyArray(mxArray* a);
 #endif
