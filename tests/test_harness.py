@@ -94,3 +94,44 @@ def test_dry_run_accepts_a_single_object(tmp_path):
     d = json.loads(out)
     assert (d["algo"], d["Ny"], d["Nx"], d["L"], d["Qy"]) == ("hs", 96, 80, 5, 1)
     assert d["pdfb_max_iter"] == 77 and d["nlevel"] == 3 and d["dr"] == 1 and d["snr_db"] == 30
+
+
+def test_matlab_wrappers_match_the_gateway_and_the_reference_signatures():
+    """Every fhs_mex command the .m wrappers call exists in the gateway, and
+    each wrapper keeps the argument list of the reference function it stands
+    in for (src/*.m, lib/operators/*.m)."""
+    import re
+    mex_dir = os.path.join(ROOT, "faceted-hypersara_b200", "mex")
+    gateway = open(os.path.join(mex_dir, "fhs_mex.c")).read()
+    commands = set(re.findall(r'!strcmp\(cmd, "(\w+)"\)', gateway))
+    expected = {
+        "apply_direct_operator": "Fx, G, Lambda",
+        "apply_adjoint_operator": "y, G, Lambda",
+        "HS_forward_operator_G": "x, G, W, A, flag_visibility_gridding, Lambda",
+        "HS_adjoint_operator_G": "y, G, W, At, N, M, flag_visibility_gridding, Lambda",
+        "proj_l2ball": "x, eps, y",
+        "nuclear_norm": "x",
+        "compute_sara_prior": "x, Psit, n_wavelet_coefficients",
+        "update_dual_data_fidelity": "v2, y, x, Fx_old, proj, A, At, G, W, pU, epsilon, elipse_proj_max_iter, "
+                                     "elipse_proj_min_iter, elipse_proj_eps, sigma22, "
+                                     "flag_dimensionality_reduction, Lambda",
+        "facetHyperSARA": "y, epsilon, A, At, pU, G, W, param, Qx, Qy, K, wavelet, filter_length, nlevel, "
+                          "window_type, spectral_chunk, n_channels, overlap_size, M, N, oy, ox, warmstart_name, "
+                          "checkpoint_name, flag_dimensionality_reduction, Lambda, varargin",
+        "hyperSARA": "y, epsilon, A, At, pU, G, W, param, K, wavelet, nlevel, spectral_chunk, n_channels, M, N, "
+                     "oy, ox, warmstart_name, checkpoint_name, flag_dimensionality_reduction, Sigma, varargin",
+        "sara": "y, epsilon, A, At, pU, G, W, Psi, Psit, param, warmstart_name, checkpoint_name, alph, "
+                "flag_dimensionality_reduction, Lambda, varargin",
+    }
+    mdir = os.path.join(mex_dir, "matlab")
+    used = set()
+    for f in sorted(os.listdir(mdir)):
+        src = open(os.path.join(mdir, f)).read()
+        used |= set(re.findall(r"fhs_mex\('(\w+)'", src))
+        name = f[:-2]
+        if name in expected:
+            head = src[:src.index(")")].replace("...", " ")
+            args = re.sub(r"\s+", " ", head[head.index(name + "(") + len(name) + 1:]).strip()
+            assert args == expected[name], (name, args)
+    assert used and used <= commands, used - commands
+    assert set(expected) <= {f[:-2] for f in os.listdir(mdir)}
