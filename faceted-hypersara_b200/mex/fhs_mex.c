@@ -26,6 +26,9 @@
  *   operator_norm       h, max_iter, tol, L                     -> nu2
  *   update_dual_data_fidelity  h, v2, y, x, Fx_old, epsilon, sigma22
  *                                  -> v2, Ftx, Fx_old, norm_res, global_norm_res, norm_epsilon
+ *   update_dual_data_fidelity_precond  h, v2, proj, y, x, Fx_old, epsilon,
+ *                                  elipse_proj_max_iter, elipse_proj_min_iter, elipse_proj_eps, sigma22
+ *                                  -> v2, Ftx, Fx_old, proj, norm_res, global_norm_res, norm_epsilon
  *   proj_l2ball         x, eps, y                               -> p
  *   nuclear_norm        x [N, L]                                -> f
  *   compute_sara_prior  x [Ny, Nx, L], nlevel                   -> f
@@ -165,6 +168,34 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         mxGetDoubles(out[3]), mxGetDoubles(out[4]), mxGetDoubles(out[5]));
     /* plhs holds max(nlhs, 1) entries: hand over the requested outputs only */
     for (int k = 0; k < 6; ++k) {
+      if (k < nlhs || k == 0)
+        plhs[k] = out[k];
+      else
+        mxDestroyArray(out[k]);
+    }
+    check(st);
+  } else if (!strcmp(cmd, "update_dual_data_fidelity_precond")) { /* src/update_dual_data_fidelity.m:126-147 */
+    need(nrhs == 12, "update_dual_data_fidelity_precond(h, v2, proj, y, x, Fx_old, epsilon, "
+                     "elipse_proj_max_iter, elipse_proj_min_iter, elipse_proj_eps, sigma22)");
+    fhs_measop* op = op_of(prhs[1]);
+    const mwSize* d = mxGetDimensions(prhs[5]);
+    (void)cplx_in(prhs[2]);  /* v2, proj and Fx_old must be complex (usage error otherwise) */
+    (void)cplx_in(prhs[3]);
+    (void)cplx_in(prhs[6]);
+    mxArray* out[7];
+    out[0] = mxDuplicateArray(prhs[2]);                                    /* v2 (updated) */
+    out[1] = mxCreateNumericArray(mxGetNumberOfDimensions(prhs[5]), d, mxDOUBLE_CLASS, mxREAL);  /* Ftx */
+    out[2] = mxDuplicateArray(prhs[6]);                                    /* Fx_old (updated) */
+    out[3] = mxDuplicateArray(prhs[3]);                                    /* proj (updated) */
+    out[4] = mxCreateDoubleMatrix(mxGetNumberOfElements(prhs[7]), 1, mxREAL); /* norm_res per block */
+    out[5] = mxCreateDoubleScalar(0.0);
+    out[6] = mxCreateDoubleScalar(0.0);
+    const fhs_status st = fhs_update_dual_data_fidelity_precond(
+        op, (double*)mxGetComplexDoubles(out[0]), (double*)mxGetComplexDoubles(out[3]), cplx_in(prhs[4]),
+        real_in(prhs[5]), (double*)mxGetComplexDoubles(out[2]), real_in(prhs[7]), (int)mxGetScalar(prhs[8]),
+        (int)mxGetScalar(prhs[9]), mxGetScalar(prhs[10]), real_in(prhs[11]), mxGetDoubles(out[1]),
+        mxGetDoubles(out[4]), mxGetDoubles(out[5]), mxGetDoubles(out[6]), NULL);
+    for (int k = 0; k < 7; ++k) {
       if (k < nlhs || k == 0)
         plhs[k] = out[k];
       else
