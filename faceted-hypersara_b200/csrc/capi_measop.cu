@@ -196,6 +196,23 @@ int64_t fhs_measop_n_vis(const fhs_measop* op, int channel) {
   return m->ch[channel].M;
 }
 
+int fhs_measop_n_blocks(const fhs_measop* op, int channel) {
+  const MeasOp* m = reinterpret_cast<const MeasOp*>(op);
+  if (!m || channel < 0 || channel >= m->L) return -1;
+  return (int)m->ch[channel].block_sizes.size();
+}
+
+fhs_status fhs_measop_image_size(const fhs_measop* op, int* Ny, int* Nx, int* n_channels) {
+  return guarded([&] {
+    const MeasOp* m = reinterpret_cast<const MeasOp*>(op);
+    FHS_CHECK(m != nullptr, FHS_ERR_INVALID_ARG, "null operator");
+    FHS_CHECK(Ny && Nx && n_channels, FHS_ERR_INVALID_ARG, "null output pointer");
+    *Ny = m->Ny;
+    *Nx = m->Nx;
+    *n_channels = m->L;
+  });
+}
+
 fhs_status fhs_measop_create_dr(fhs_measop* vis, fhs_measop** out) {
   return guarded([&] {
     FHS_CHECK(out != nullptr, FHS_ERR_INVALID_ARG, "null output handle");

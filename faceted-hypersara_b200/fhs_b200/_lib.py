@@ -80,6 +80,8 @@ SIGNATURES = {
     "fhs_measop_dr_cells": (C.c_int, [_vp, C.c_int, _i64p]),
     "fhs_measop_dr_lambda": (C.c_int, [_vp, C.c_int, _dp]),
     "fhs_measop_grid_size": (C.c_int64, [_vp]),
+    "fhs_measop_n_blocks": (C.c_int, [_vp, C.c_int]),
+    "fhs_measop_image_size": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "fhs_scaled_fft": (C.c_int, [_vp, _dp, _dp]),
     "fhs_scaled_fft_adjoint": (C.c_int, [_vp, _dp, _dp]),
     "fhs_apply_direct_operator": (C.c_int, [_vp, C.c_int, _dp, _dp]),

@@ -86,6 +86,32 @@ static int64_t total_vis(fhs_measop* op, int L) {
   return n;
 }
 
+/* Sizes every operand of an operator call must have: the library reads and
+ * writes exactly these counts, so a short MATLAB array is a usage error here
+ * instead of a heap overrun inside the MATLAB process. */
+typedef struct {
+  int Ny, Nx, L;
+  int64_t n_vis;   /* all channels */
+  int64_t n_blk;   /* all channels */
+  int64_t No;
+} op_shape;
+
+static op_shape shape_of(fhs_measop* op) {
+  op_shape sh;
+  memset(&sh, 0, sizeof sh);
+  check(fhs_measop_image_size(op, &sh.Ny, &sh.Nx, &sh.L));
+  for (int l = 0; l < sh.L; ++l) {
+    sh.n_vis += fhs_measop_n_vis(op, l);
+    sh.n_blk += fhs_measop_n_blocks(op, l);
+  }
+  sh.No = fhs_measop_grid_size(op);
+  return sh;
+}
+
+static void need_numel(const mxArray* a, int64_t n, const char* msg) {
+  need((int64_t)mxGetNumberOfElements(a) == n, msg);
+}
+
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   char cmd[64];
   need(nrhs >= 1 && mxIsChar(prhs[0]) && mxGetString(prhs[0], cmd, sizeof cmd) == 0, "first input: command");
@@ -102,6 +128,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     const mwSize n = mxGetNumberOfElements(prhs[3]);
     const mwSize nb = mxGetNumberOfElements(prhs[6]);
     need(nb >= 1 && nb <= 16, "1 to 16 blocks");
+    need(mxGetNumberOfElements(prhs[4]) == n, "om_x: same size as om_y");
+    need(mxIsEmpty(prhs[5]) || mxGetNumberOfElements(prhs[5]) == n, "weights: [] or one per visibility");
     int64_t bs[16];
     const double* b = real_in(prhs[6]);
     for (mwSize k = 0; k < nb; ++k) bs[k] = (int64_t)b[k];
@@ -116,30 +144,46 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     check(fhs_measop_create_dr(op_of(prhs[1]), &dr));
     plhs[0] = handle_out(dr);
   } else if (!strcmp(cmd, "measop_set_preconditioner")) {
-    check(fhs_measop_set_preconditioner(op_of(prhs[1]), (int)mxGetScalar(prhs[2]), real_in(prhs[3])));
+    need(nrhs == 4, "measop_set_preconditioner(h, l, pU)");
+    fhs_measop* op = op_of(prhs[1]);
+    const int ch = (int)mxGetScalar(prhs[2]);
+    need(fhs_measop_n_vis(op, ch) >= 0, "channel out of range");
+    need_numel(prhs[3], fhs_measop_n_vis(op, ch), "pU: one entry per visibility of the channel");
+    check(fhs_measop_set_preconditioner(op, ch, real_in(prhs[3])));
   } else if (!strcmp(cmd, "measop_n_vis")) {
     plhs[0] = mxCreateDoubleScalar((double)fhs_measop_n_vis(op_of(prhs[1]), (int)mxGetScalar(prhs[2])));
   } else if (!strcmp(cmd, "apply_direct_operator")) { /* src/apply_direct_operator.m:1 */
+    need(nrhs == 4, "apply_direct_operator(h, l, Fx)");
     fhs_measop* op = op_of(prhs[1]);
     const int ch = (int)mxGetScalar(prhs[2]);
+    need(fhs_measop_n_vis(op, ch) >= 0, "channel out of range");
+    need_numel(prhs[3], fhs_measop_grid_size(op), "Fx: one entry per grid point (No = Ky*Kx)");
     plhs[0] = mxCreateDoubleMatrix((mwSize)fhs_measop_n_vis(op, ch), 1, mxCOMPLEX);
     check(fhs_apply_direct_operator(op, ch, cplx_in(prhs[3]), (double*)mxGetComplexDoubles(plhs[0])));
   } else if (!strcmp(cmd, "apply_adjoint_operator")) { /* src/apply_adjoint_operator.m:1 */
+    need(nrhs == 4, "apply_adjoint_operator(h, l, y)");
     fhs_measop* op = op_of(prhs[1]);
+    const int ch = (int)mxGetScalar(prhs[2]);
+    need(fhs_measop_n_vis(op, ch) >= 0, "channel out of range");
+    need_numel(prhs[3], fhs_measop_n_vis(op, ch), "y: one entry per visibility of the channel");
     plhs[0] = mxCreateDoubleMatrix((mwSize)fhs_measop_grid_size(op), 1, mxCOMPLEX);
     check(fhs_apply_adjoint_operator(op, (int)mxGetScalar(prhs[2]), cplx_in(prhs[3]),
                                      (double*)mxGetComplexDoubles(plhs[0])));
   } else if (!strcmp(cmd, "HS_forward_operator_G")) { /* lib/operators/HS_forward_operator_G.m */
+    need(nrhs == 3, "HS_forward_operator_G(h, x)");
     fhs_measop* op = op_of(prhs[1]);
-    const mwSize* d = mxGetDimensions(prhs[2]);
-    const int L = mxGetNumberOfDimensions(prhs[2]) > 2 ? (int)d[2] : 1;
-    plhs[0] = mxCreateDoubleMatrix((mwSize)total_vis(op, L), 1, mxCOMPLEX);
+    const op_shape sh = shape_of(op);
+    need_numel(prhs[2], (int64_t)sh.Ny * sh.Nx * sh.L, "x: [Ny, Nx, L] of the operator");
+    plhs[0] = mxCreateDoubleMatrix((mwSize)total_vis(op, sh.L), 1, mxCOMPLEX);
     check(fhs_forward_operator(op, real_in(prhs[2]), (double*)mxGetComplexDoubles(plhs[0])));
   } else if (!strcmp(cmd, "HS_adjoint_operator_G")) { /* lib/operators/HS_adjoint_operator_G.m, then real() */
     need(nrhs == 4, "HS_adjoint_operator_G(h, y, [Ny Nx L])");
     fhs_measop* op = op_of(prhs[1]);
     need(mxGetNumberOfElements(prhs[3]) == 3, "cube size [Ny Nx L]");
     const double* sz = real_in(prhs[3]);
+    const op_shape sh = shape_of(op);
+    need(sz[0] == sh.Ny && sz[1] == sh.Nx && sz[2] == sh.L, "cube size [Ny Nx L] of the operator");
+    need_numel(prhs[2], sh.n_vis, "y: all channels' visibilities");
     const mwSize dims[3] = {(mwSize)sz[0], (mwSize)sz[1], (mwSize)sz[2]};
     plhs[0] = mxCreateNumericArray(3, dims, mxDOUBLE_CLASS, mxREAL);
     check(fhs_adjoint_operator(op, cplx_in(prhs[2]), mxGetDoubles(plhs[0])));
@@ -147,6 +191,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     need(nrhs == 5, "operator_norm(h, max_iter, tol, L)");
     fhs_measop* op = op_of(prhs[1]);
     const int L = (int)mxGetScalar(prhs[4]);
+    need(L == shape_of(op).L, "L: the operator's channel count");
     plhs[0] = mxCreateDoubleMatrix((mwSize)L, 1, mxREAL);
     check(fhs_operator_norm(op, (int)mxGetScalar(prhs[2]), mxGetScalar(prhs[3]), mxGetDoubles(plhs[0])));
   } else if (!strcmp(cmd, "update_dual_data_fidelity")) { /* src/update_dual_data_fidelity.m:1-6 */
@@ -155,6 +200,15 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     const mwSize* d = mxGetDimensions(prhs[4]);
     (void)cplx_in(prhs[2]);  /* v2 and Fx_old must be complex (usage error otherwise) */
     (void)cplx_in(prhs[5]);
+    {
+      const op_shape sh = shape_of(op);
+      need_numel(prhs[2], sh.n_vis, "v2: all channels' visibilities");
+      need_numel(prhs[3], sh.n_vis, "y: all channels' visibilities");
+      need_numel(prhs[4], (int64_t)sh.Ny * sh.Nx * sh.L, "x: [Ny, Nx, L] of the operator");
+      need_numel(prhs[5], sh.No * sh.L, "Fx_old: [No, L]");
+      need_numel(prhs[6], sh.n_blk, "epsilon: one bound per block");
+      need_numel(prhs[7], sh.L, "sigma22: one per channel");
+    }
     mxArray* out[6];
     out[0] = mxDuplicateArray(prhs[2]);                                    /* v2 (updated) */
     out[1] = mxCreateNumericArray(mxGetNumberOfDimensions(prhs[4]), d, mxDOUBLE_CLASS, mxREAL);  /* Ftx */
@@ -182,6 +236,16 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     (void)cplx_in(prhs[2]);  /* v2, proj and Fx_old must be complex (usage error otherwise) */
     (void)cplx_in(prhs[3]);
     (void)cplx_in(prhs[6]);
+    {
+      const op_shape sh = shape_of(op);
+      need_numel(prhs[2], sh.n_vis, "v2: all channels' visibilities");
+      need_numel(prhs[3], sh.n_vis, "proj: all channels' visibilities");
+      need_numel(prhs[4], sh.n_vis, "y: all channels' visibilities");
+      need_numel(prhs[5], (int64_t)sh.Ny * sh.Nx * sh.L, "x: [Ny, Nx, L] of the operator");
+      need_numel(prhs[6], sh.No * sh.L, "Fx_old: [No, L]");
+      need_numel(prhs[7], sh.n_blk, "epsilon: one bound per block");
+      need_numel(prhs[11], sh.L, "sigma22: one per channel");
+    }
     mxArray* out[7];
     out[0] = mxDuplicateArray(prhs[2]);                                    /* v2 (updated) */
     out[1] = mxCreateNumericArray(mxGetNumberOfDimensions(prhs[5]), d, mxDOUBLE_CLASS, mxREAL);  /* Ftx */
@@ -203,7 +267,9 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     }
     check(st);
   } else if (!strcmp(cmd, "proj_l2ball")) { /* src/proj_l2ball.m:1 */
+    need(nrhs == 4, "proj_l2ball(x, eps, y)");
     const mwSize n = mxGetNumberOfElements(prhs[1]);
+    need(mxGetNumberOfElements(prhs[3]) == n, "y: same size as x");
     plhs[0] = mxCreateDoubleMatrix(n, 1, mxCOMPLEX);
     check(fhs_proj_l2ball(0, (int64_t)n, cplx_in(prhs[1]), mxGetScalar(prhs[2]), cplx_in(prhs[3]),
                           (double*)mxGetComplexDoubles(plhs[0])));
@@ -237,6 +303,15 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     cfg.overlap_x = (int)field_num(cfg_s, "overlap_x", 0);
     cfg.window = (int)field_num(cfg_s, "window", cfg.algo == FHS_ALGO_FHS ? FHS_WINDOW_TRIANGULAR : FHS_WINDOW_NONE);
     const int L = (int)field_num(cfg_s, "L", 1);
+    {
+      const op_shape sh = shape_of(op);
+      need(L == sh.L && (int)field_num(cfg_s, "Ny", 0) == sh.Ny && (int)field_num(cfg_s, "Nx", 0) == sh.Nx,
+           "cfg.Ny, cfg.Nx, cfg.L: the operator's image size and channel count");
+      need_numel(prhs[5], sh.n_vis, "y: all channels' visibilities");
+      need_numel(prhs[6], sh.n_blk, "epsilon: one bound per block");
+      need(mxIsEmpty(prhs[7]) || (int64_t)mxGetNumberOfElements(prhs[7]) == (int64_t)sh.Ny * sh.Nx * sh.L,
+           "xinit: [] or [Ny, Nx, L]");
+    }
     const int G = cfg.algo == FHS_ALGO_SARA ? L : cfg.n_groups;
     const int Q = cfg.algo == FHS_ALGO_FHS ? cfg.Qy * cfg.Qx : 1;
     fhs_solver_params p;

@@ -78,6 +78,12 @@ FHS_API fhs_status fhs_measop_set_channel(fhs_measop* op, int channel, int64_t n
 FHS_API fhs_status fhs_measop_commit(fhs_measop* op);
 FHS_API int64_t fhs_measop_n_vis(const fhs_measop* op, int channel);
 FHS_API int64_t fhs_measop_grid_size(const fhs_measop* op); /* No = Ky*Kx */
+/* Blocks of a channel as set by fhs_measop_set_channel (-1: bad channel);
+ * the cell {l}{b} count of y / epsilon in update_dual_data_fidelity.m:1-6. */
+FHS_API int fhs_measop_n_blocks(const fhs_measop* op, int channel);
+/* Image size [Ny, Nx] and channel count L of x in the calls below (the
+ * [M, N, L] of facetHyperSARA.m:1-6); host-side, needs no device. */
+FHS_API fhs_status fhs_measop_image_size(const fhs_measop* op, int* Ny, int* Nx, int* n_channels);
 
 /* A (op_nufft's scaled zero-padded FFT; shape contract of
  * src/apply_scaled_fourier_transform.m:21-24): x[Ny,Nx] -> Fx[No] complex. */

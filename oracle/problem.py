@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from ._par import pmap
 from .nufft import NufftOperator
 from .solvers import DataTerm
 
@@ -27,20 +28,26 @@ def make_problem(Ny, Nx, L, M_per_channel, n_blocks, seed, snr_db=40.0, synth=No
     nu = synth.frequencies(L)
     rng = np.random.default_rng(seed + 31)
     G_all, y_all, eps_all, meta = [], [], [], {"om": [], "blocks": [], "sigma": []}
-    for l in range(L):
+
+    def build(l):   # no random draws here: the seeded stream below stays in channel order
         oy, ox = synth.channel_coverage(om_y0[: Ms[l]], om_x0[: Ms[l]], nu[l], nu[-1])
-        sizes = synth.split_blocks(Ms[l], nbs[l], rng)
         G = op.G(oy, ox)
-        y0 = G @ op.A(x[l])
+        return oy, ox, G, G @ op.A(x[l])
+    built = pmap(build, range(L))
+    for l in range(L):
+        oy, ox, G, y0 = built[l]
+        built[l] = None   # large sizes: hold one channel's full G at a time besides the blocks
+        sizes = synth.split_blocks(Ms[l], nbs[l], rng)
         sigma = synth.noise_sigma(y0, snr_db)
         yl = (y0 + sigma * synth.noise(Ms[l], rng)) / sigma
-        Gw = G / sigma
+        G.data /= sigma   # whitening, in place
         Gb, yb = [], []
         pos = 0
         for m in sizes:
-            Gb.append(Gw[pos:pos + m])
+            Gb.append(G[pos:pos + m] if len(sizes) > 1 else G)
             yb.append(yl[pos:pos + m])
             pos += m
+        del G
         G_all.append(Gb)
         y_all.append(yb)
         eps_all.append(synth.l2_bounds(sizes))

@@ -24,10 +24,17 @@ import numpy as np
 from scipy.special import gammaln
 
 from . import wavelets as wv
+from ._par import pmap
 from .facets import FacetGeometry
 from .nufft import NufftOperator
 
 MATLAB_EPS = np.finfo(np.float64).eps
+
+
+def _adj(G, v):
+    """G' v without copying G: conj(G^T conj(v)) (bit-identical to
+    G.conj().T @ v: conjugation is exact and the sums run in the same order)."""
+    return np.conj(G.T @ np.conj(v))
 
 
 # ----------------------------------------------------------------- small ops
@@ -74,27 +81,25 @@ class DataTerm:
 def forward_operator(x, data: DataTerm, pU=None):
     """lib/operators/HS_forward_operator_G.m:36-52 (no DR); with pU,
     HS_forward_operator_precond_G.m:40-55: sqrt(pU) .* (G A x)."""
-    out = []
-    for l in range(data.L):
+    def one(l):
         Fx = data.op.A(x[l])
         if pU is None:
-            out.append([G @ Fx for G in data.G[l]])
-        else:
-            out.append([np.sqrt(pu) * (G @ Fx) for G, pu in zip(data.G[l], pU[l])])
-    return out
+            return [G @ Fx for G in data.G[l]]
+        return [np.sqrt(pu) * (G @ Fx) for G, pu in zip(data.G[l], pU[l])]
+    return pmap(one, range(data.L))
 
 
 def adjoint_operator(yb, data: DataTerm, pU=None):
     """lib/operators/HS_adjoint_operator_G.m:42-57 (no DR), real part kept;
     with pU, HS_adjoint_operator_precond_G.m: At(G' (sqrt(pU) .* y))."""
     op = data.op
-    out = np.zeros((data.L, op.Ny, op.Nx))
-    for l in range(data.L):
+
+    def one(l):
         g2 = np.zeros(op.No, dtype=np.complex128)
         for b, (G, v) in enumerate(zip(data.G[l], yb[l])):
-            g2 += G.conj().T @ (v if pU is None else np.sqrt(pU[l][b]) * v)
-        out[l] = np.real(op.At(g2))
-    return out
+            g2 += _adj(G, v if pU is None else np.sqrt(pU[l][b]) * v)
+        return np.real(op.At(g2))
+    return np.stack(pmap(one, range(data.L))).reshape(data.L, op.Ny, op.Nx)
 
 
 def uniform_weight_preconditioner(om_y, om_x, Ky, Kx):
@@ -139,10 +144,9 @@ def update_dual_data_fidelity_precond(v2, proj, x, Fx_old, data: DataTerm, pU, s
     global_norm_res^2, norm_epsilon^2)."""
     op = data.op
     Ftx = np.zeros_like(x)
-    norm_res, v2n, pn = [], [], []
-    gres, geps = 0.0, 0.0
     Fx_new = np.empty_like(Fx_old)
-    for l in range(data.L):
+
+    def one(l):
         Fx = op.A(x[l])
         g2 = np.zeros(op.No, dtype=np.complex128)
         nr, vl, pl = [], [], []
@@ -153,16 +157,22 @@ def update_dual_data_fidelity_precond(v2, proj, x, Fx_old, data: DataTerm, pU, s
             vb = v2[l][b] + pU[l][b] * (r2 - p)
             vl.append(vb)
             pl.append(p)
-            g2 += G.conj().T @ vb
-            res = np.linalg.norm(G @ Fx - data.y[l][b])
-            nr.append(res)
+            g2 += _adj(G, vb)
+            nr.append(np.linalg.norm(G @ Fx - data.y[l][b]))
+        return Fx, vl, pl, nr, sigma22[l] * np.real(op.At(g2))
+
+    outs = pmap(one, range(data.L))
+    norm_res, v2n, pn = [], [], []
+    gres, geps = 0.0, 0.0
+    for l, (Fx, vl, pl, nr, ftx) in enumerate(outs):   # channel and block order
+        for b, res in enumerate(nr):
             gres += res ** 2
             geps += data.eps[l][b] ** 2
         v2n.append(vl)
         pn.append(pl)
         norm_res.append(nr)
         Fx_new[l] = Fx
-        Ftx[l] = sigma22[l] * np.real(op.At(g2))
+        Ftx[l] = ftx
     return v2n, pn, Ftx, Fx_new, norm_res, gres, geps
 
 
@@ -173,11 +183,9 @@ def update_dual_data_fidelity(v2, x, Fx_old, data: DataTerm, sigma22):
     """
     op = data.op
     Ftx = np.zeros_like(x)
-    norm_res = []
-    gres, geps = 0.0, 0.0
     Fx_new = np.empty_like(Fx_old)
-    v2n = []
-    for l in range(data.L):
+
+    def one(l):
         Fx = op.A(x[l])
         g2 = np.zeros(op.No, dtype=np.complex128)
         nr, vl = [], []
@@ -186,15 +194,21 @@ def update_dual_data_fidelity(v2, x, Fx_old, data: DataTerm, sigma22):
             p = proj_l2ball(v2[l][b] + r2, data.eps[l][b], data.y[l][b])
             vb = v2[l][b] + r2 - p
             vl.append(vb)
-            g2 += G.conj().T @ vb
-            res = np.linalg.norm(G @ Fx - data.y[l][b])
-            nr.append(res)
+            g2 += _adj(G, vb)
+            nr.append(np.linalg.norm(G @ Fx - data.y[l][b]))
+        return Fx, vl, nr, sigma22[l] * np.real(op.At(g2))
+
+    outs = pmap(one, range(data.L))
+    norm_res, v2n = [], []
+    gres, geps = 0.0, 0.0
+    for l, (Fx, vl, nr, ftx) in enumerate(outs):   # channel and block order
+        for b, res in enumerate(nr):
             gres += res ** 2
             geps += data.eps[l][b] ** 2
         v2n.append(vl)
         norm_res.append(nr)
         Fx_new[l] = Fx
-        Ftx[l] = sigma22[l] * np.real(op.At(g2))
+        Ftx[l] = ftx
     return v2n, Ftx, Fx_new, norm_res, gres, geps
 
 
@@ -206,17 +220,20 @@ def compute_residual_images(x, data: DataTerm):
     out = np.zeros_like(x)
     dirac = np.zeros((op.Ny, op.Nx))
     dirac[op.Ny // 2, op.Nx // 2] = 1.0
-    for l in range(data.L):
+
+    def one(l):
         Fx = op.A(x[l])
         r = np.zeros(op.No, dtype=np.complex128)
         for G, yb in zip(data.G[l], data.y[l]):
-            r += G.conj().T @ (yb - G @ Fx)
+            r += _adj(G, yb - G @ Fx)
         res = np.real(op.At(r))
         Fd = op.A(dirac)
         rp = np.zeros(op.No, dtype=np.complex128)
         for G in data.G[l]:
-            rp += G.conj().T @ (G @ Fd)
-        out[l] = res / np.max(np.real(op.At(rp)))
+            rp += _adj(G, G @ Fd)
+        return res / np.max(np.real(op.At(rp)))
+    for l, r in enumerate(pmap(one, range(data.L))):
+        out[l] = r
     return out
 
 
@@ -226,16 +243,16 @@ def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0, pU=None):
     with pU, of sqrt(pU) G_l A (util_operator_norm.m:46-52)."""
     rng = np.random.default_rng(seed)
     op = data.op
-    out = np.zeros(data.L)
-    for l in range(data.L):
-        x = rng.standard_normal((op.Ny, op.Nx))
-        x /= np.linalg.norm(x)
+    starts = [rng.standard_normal((op.Ny, op.Nx)) for _ in range(data.L)]   # drawn in channel order
+
+    def one(l):
+        x = starts[l] / np.linalg.norm(starts[l])
         val = 0.0
         for _ in range(n_iter):
             Fx = op.A(x)
             g2 = np.zeros(op.No, dtype=np.complex128)
             for b, G in enumerate(data.G[l]):
-                g2 += G.conj().T @ (G @ Fx if pU is None else pU[l][b] * (G @ Fx))
+                g2 += _adj(G, G @ Fx if pU is None else pU[l][b] * (G @ Fx))
             xn = np.real(op.At(g2))
             new = np.linalg.norm(xn)
             x = xn / new
@@ -243,8 +260,8 @@ def operator_norm(data: DataTerm, n_iter=200, tol=1e-8, seed=0, pU=None):
                 val = new
                 break
             val = new
-        out[l] = val
-    return out
+        return val
+    return np.array(pmap(one, range(data.L)), dtype=np.float64)
 
 
 # ---------------------------------------------------------------- the priors
@@ -446,8 +463,10 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
         x, xhat, rel_x, norm_x = primal_update(x, g)
         v2, proj, Ftx, Fx_old, gres, geps, nres = _dual_step(v2, proj, x, Fx_old, data, sigma22, precond)
         gacc = np.zeros_like(x)
-        for q, (y0, y1), (x0, x1), win in facets:
-            v0[q], g0 = nuclear_prox_update(v0[q], xhat[:, y0:y1, x0:x1], win, w0[q], beta0[q])
+        prox = pmap(lambda f: nuclear_prox_update(v0[f[0]], xhat[:, f[1][0]:f[1][1], f[2][0]:f[2][1]], f[3],
+                                                  w0[f[0]], beta0[f[0]]), facets)
+        for (q, (y0, y1), (x0, x1), win), (v0q, g0) in zip(facets, prox):   # overlaps summed in facet order
+            v0[q] = v0q
             gacc[:, y0:y1, x0:x1] += sigma00 * g0
         v1, g1 = l21_prox_update(v1, xhat, w1, beta1, p.nlevel)
         g = gacc + sigma11 * g1 + Ftx

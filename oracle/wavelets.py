@@ -37,6 +37,8 @@ from math import comb
 
 import numpy as np
 
+from ._par import pmap
+
 SARA_WAVELETS = ("db1", "db2", "db3", "db4", "db5", "db6", "db7", "db8")
 N_BASES = len(SARA_WAVELETS) + 1   # + Dirac ("self")
 
@@ -185,20 +187,51 @@ def waverec2(c: np.ndarray, n0: int, n1: int, nlevel: int, name: str) -> np.ndar
     return a
 
 
+def _channel_chunks(lead, plane=None, min_elems=1 << 19):
+    """Slices of the leading (channel) axis for threaded SARA transforms, or
+    None to run sequentially (small transforms: thread overhead dominates)."""
+    if len(lead) != 1:
+        return None
+    L = lead[0]
+    if plane is not None and L * plane < min_elems:
+        return None
+    from ._par import n_threads
+    k = max(1, min(L, n_threads() // 2))
+    edges = [round(i * L / k) for i in range(k + 1)]
+    return [slice(a, b) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+
+
 def sara_analysis(x: np.ndarray, nlevel: int = 4) -> np.ndarray:
     """Psit: x [..., n0, n1] -> [..., s], s = n_coefs_sara(n0, n1, nlevel)."""
-    parts = [wavedec2(x, nlevel, w) for w in SARA_WAVELETS] + [_vec(x)]
+    chunks = _channel_chunks(x.shape[:-2], x.shape[-2] * x.shape[-1])
+    if chunks is None:
+        parts = [wavedec2(x, nlevel, w) for w in SARA_WAVELETS]
+    else:   # (basis, channel chunk) jobs on the oracle's threads
+        jobs = [(w, c) for w in SARA_WAVELETS for c in chunks]
+        res = pmap(lambda j: wavedec2(x[j[1]], nlevel, j[0]), jobs)
+        parts = [np.concatenate(res[i * len(chunks):(i + 1) * len(chunks)], axis=0)
+                 for i in range(len(SARA_WAVELETS))]
+    parts.append(_vec(x))
     return np.concatenate(parts, axis=-1) / np.sqrt(N_BASES)
 
 
 def sara_synthesis(c: np.ndarray, n0: int, n1: int, nlevel: int = 4) -> np.ndarray:
     """Psi: [..., s] -> [..., n0, n1] (adjoint of ``sara_analysis``)."""
-    out = 0.0
-    pos = 0
+    jobs, pos = [], 0
     for w in SARA_WAVELETS:
         sb = n_coefs_basis(n0, n1, 2 * int(w[2:]), nlevel)
-        out = out + waverec2(c[..., pos:pos + sb], n0, n1, nlevel, w)
+        jobs.append((w, pos, sb))
         pos += sb
+    chunks = _channel_chunks(c.shape[:-1], n0 * n1)
+    if chunks is None:
+        recs = [waverec2(c[..., p0:p0 + sb], n0, n1, nlevel, w) for w, p0, sb in jobs]
+    else:   # (basis, channel chunk) jobs on the oracle's threads
+        res = pmap(lambda j: waverec2(c[j[1]][..., j[0][1]:j[0][1] + j[0][2]], n0, n1, nlevel, j[0][0]),
+                   [(b, ch) for b in jobs for ch in chunks])
+        recs = [np.concatenate(res[i * len(chunks):(i + 1) * len(chunks)], axis=0) for i in range(len(jobs))]
+    out = 0.0
+    for r in recs:   # summed in basis order, as the sequential form
+        out = out + r
     out = out + _unvec(c[..., pos:pos + n0 * n1], n0, n1)
     return out / np.sqrt(N_BASES)
 
