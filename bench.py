@@ -158,7 +158,6 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
     ov = prob["overlap"][0]
     from fhs_b200.heuristics import facet_pixels
     P = sum(facet_pixels(sy, sx, (ov, ov)))
-    s_w = sp_s - N
     pre = 20 if prob.get("precond") else 0
     if prob.get("dr"):
         # DR apply passes: the 85-entry c64 half stencil and the weight (c64)
@@ -173,8 +172,9 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
         "primal_pad": N * L * (4 + 4) + N * L * (4 + 4 + 8),
         "degrid_dual": No * L * 8 + M * (16 + 8 + 8 + 8 + pre) + M * (8 + 8),
         "grid_dual": M * (16 + 8 + pre) + M * 8 + No * L * 8,
-        "sara_analysis": N * L * 4 + s_w * L * 4,
-        "l21_prox": 2 * sp_s * L * 4 + s_w * L * 4 + N * L * 4 + sp_s * 4 * prob["C"],
+        # fused analysis + weighted l21 prox (Dirac part included): read
+        # x-hat, read and write v1 (all s coefficients), read weights1 per group
+        "sara_analysis_prox": N * L * 4 + 2 * sp_s * L * 4 + sp_s * 4 * prob["C"],
         "sara_synthesis": sp_s * L * 4 + N * L * 4,
         "facet_gram": 2 * P * L * 4,
         "facet_reconstruct": 3 * P * L * 4,
@@ -187,60 +187,60 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
     return out
 
 
-def _traffic_from_profiles(kernel):
-    """dram bytes per launch of `kernel` from a committed ncu summary, if any."""
-    d = os.path.join(ROOT, "profiles")
-    if not os.path.isdir(d):
-        return None
-    for f in sorted(os.listdir(d)):
-        if not f.startswith(kernel) or not f.endswith(".md"):
-            continue
-        with open(os.path.join(d, f)) as fh:
-            for line in fh:
-                if line.strip().startswith("dram_bytes_per_launch_full ="):
-                    try:
-                        return float(line.split("=")[1].split()[0])
-                    except Exception:
-                        return None
-    return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of a
+# stage at the bench workload, from one ncu capture of the current kernels
+# (the medium case, 512 x 512 x 64, scaled by 4: grid cells, visibilities,
+# pixels and coefficients all grow by 4 to 1024 x 1024 x 64).  A stage
+# without a capture of its current code reports traffic null.
+TRAFFIC_PER_LAUNCH = {}
 
 
-def _cpu_sample(seed=0):
-    """The oracle's bounded sample of the workload: one channel of one
-    sub-cube at full resolution (1024 x 1024, all of that channel's
-    visibilities, 4x4 facets); returns a function running one FHS iteration
-    (FP64 NumPy/SciPy, all host threads)."""
+def _cpu_sample(wl, seed=0):
+    """The oracle's bounded sample of the workload: one spectral sub-cube
+    (L / C = 16 channels of the 1024 x 1024 cube, every one of their
+    visibilities in 2-6 blocks, 4 x 4 jittered facets with 10% overlap), with
+    every coupling of an iteration: the L x L facet SVDs of the nuclear prior
+    and the l21 prior across the sub-cube's channels.  Returns a function
+    running one FHS iteration (FP64 NumPy/SciPy on all host threads).  The
+    regularisation parameters are fixed values: an iteration's cost does not
+    depend on them."""
     import numpy as np
 
     from fhs_b200 import synth
+    from oracle import problem
     from oracle import solvers as so
     from oracle.facets import FacetGeometry
-    from oracle.nufft import NufftOperator
     rng = np.random.default_rng(seed)
-    Ny = Nx = WORKLOAD["Ny"]
+    Ny, Nx, lg = wl["Ny"], wl["Nx"], wl["L"] // wl["C"]
     N = Ny * Nx
-    M = int(rng.integers(int(0.3 * N), N + 1))
-    x = synth.sky_image(Ny, Nx, seed)[None]
-    om_y, om_x = synth.base_coverage(M, seed)
-    op = NufftOperator(Ny, Nx)
-    G = op.G(om_y, om_x)
-    y = [G @ op.A(x[0])]
-    data = so.DataTerm(op, [[G]], [y], [[float(np.sqrt(M + 2 * np.sqrt(M)))]])
-    geom = FacetGeometry(Ny, Nx, 4, 4, (26, 26))
-    p = so.SolverParams(nu2=np.array([1e3]), gamma=1e-3, gamma0=np.full(16, 1e-2), reweighting_sig=1e-3,
-                        reweighting_sig_bar=np.full(16, 1e-2), pdfb_min_iter=10 ** 6, reweighting_flag=False)
-    return lambda: so.facet_hypersara(data, p, geom, max_iter=1)
+    Ms = [int(m) for m in rng.integers(int(wl["m_lo"] * N), int(wl["m_hi"] * N) + 1, size=lg)]
+    nbs = [int(b) for b in rng.integers(wl["blocks"][0], wl["blocks"][1] + 1, size=lg)]
+    data, _, _ = problem.make_problem(Ny, Nx, lg, Ms, nbs, seed, synth=synth)
+    ov = int(round(wl["overlap_frac"] * min(Ny, Nx) / wl["Q"]))
+    geom = FacetGeometry(Ny, Nx, wl["Q"], wl["Q"], (ov, ov), splits_y=synth.jittered_splits(wl["Q"], Ny, 0.15, rng),
+                         splits_x=synth.jittered_splits(wl["Q"], Nx, 0.15, rng))
+    p = so.SolverParams(nu2=np.full(lg, 1e5), gamma=1e-3, gamma0=np.full(geom.Q, 1e-2), reweighting_sig=1e-3,
+                        reweighting_sig_bar=np.full(geom.Q, 1e-2))
+    it = so.FhsIteration(data, p, geom)
+    return it.step, sum(Ms)
 
 
-def cpu_sample_seconds(seed=0, n_iter=1):
-    """Seconds of one oracle FHS iteration on the sample of _cpu_sample (after
-    one untimed iteration); the whole-cube estimate scales it by 64 channels."""
-    step = _cpu_sample(seed)
+def _sample_text(wl, n_vis):
+    lg = wl["L"] // wl["C"]
+    return (f"one FHS iteration of the FP64 oracle on one spectral sub-cube ({wl['Ny']}x{wl['Nx']}x{lg}, "
+            f"{n_vis} visibilities, {wl['Q']}x{wl['Q']} facets: all data terms, the {lg}-channel facet SVDs and "
+            f"the l21 prior), x{wl['C']} sub-cubes for the whole cube")
+
+
+def cpu_sample_seconds(wl, n_iter=1, seed=0):
+    """Seconds of one oracle iteration of the sub-cube sample (after one
+    untimed iteration) and the sample's description."""
+    step, n_vis = _cpu_sample(wl, seed)
     step()   # warm-up (allocations, FFT plans)
     t0 = time.perf_counter()
     for _ in range(n_iter):
         step()
-    return (time.perf_counter() - t0) / n_iter
+    return (time.perf_counter() - t0) / n_iter, _sample_text(wl, n_vis)
 
 
 def _ncores():
@@ -250,27 +250,37 @@ def _ncores():
         return os.cpu_count() or 1
 
 
+REFERENCE_BUDGET_S = 150.0
+
+
 def run_reference(args):
+    """The reference arm: the FP64 oracle (a port: the MATLAB reference cannot
+    run here) timed on the host cores over the sub-cube sample.  One untimed
+    warm-up iteration (FFT plans, allocations), then up to --steps timed
+    iterations, stopping early once REFERENCE_BUDGET_S seconds are spent so
+    that the run stays within a few minutes; `steps` reports the count timed."""
     world, rank, local = _dist()
     if rank != 0:
         return 0
-    os.environ.setdefault("OMP_NUM_THREADS", str(_ncores()))
-    L = WORKLOAD["L"]
-    step = _cpu_sample(0)   # built once; each step is one oracle iteration on it
+    wl = {"small": SMALL, "medium": MEDIUM}.get(args.case, WORKLOAD)
+    step, n_vis = _cpu_sample(wl, 0)
+    step()
     times = []
-    for i in range(args.warmup + args.steps):
+    t_start = time.perf_counter()
+    for _ in range(args.steps):
         t0 = time.perf_counter()
         step()
-        if i >= args.warmup:
-            times.append(time.perf_counter() - t0)
-    per_cube = sum(times) / len(times) * L
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > REFERENCE_BUDGET_S:
+            break
+    per_cube = sum(times) / len(times) * wl["C"]
     value = 1.0 / per_cube
-    sample = (f"one FHS iteration of the FP64 oracle on 1 channel (1024x1024, its full visibility set, 4x4 "
-              f"facets), x{L} channels for the whole cube; {args.steps} steps")
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": per_cube * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": _config({"reference": "oracle port (MATLAB reference not runnable here)"}),
+    sample = _sample_text(wl, n_vis) + f"; {len(times)} timed iterations after 1 warm-up"
+    cfg = _config({"reference": "FP64 oracle port (MATLAB reference not runnable here)"}) if args.case == "full" \
+        else {"workload": f"fhs_{wl['Ny']}x{wl['Nx']}x{wl['L']}_C{wl['C']}_Q4x4 (profiling case)"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+            "warmup": 1, "ms_per_step": per_cube * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": _ncores(), "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -349,7 +359,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                 "algorithmic_bytes": nbytes[dom], "ms_per_launch": mine[dom],
-                "traffic": _traffic_from_profiles("dr_apply" if args.dr else dom)}
+                "traffic": None if (args.dr or args.case != "full") else TRAFFIC_PER_LAUNCH.get(dom)}
     stage_rows = {k: {"ms": round(v, 4), **({"gbs": round(nbytes[k] / (v / 1e3) / 1e9, 1)} if k in nbytes and v > 0
                                            else {})} for k, v in stages.items()}
     # ---- end to end through the public API with pinned host buffers
@@ -366,10 +376,9 @@ def run_ours(args):
                        "fhs_solver_get_x, host wall clock"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.case == "full":
-        t = cpu_sample_seconds()
-        cpu = {"value": 1.0 / (t * WORKLOAD["L"]), "unit": UNIT, "cores": _ncores(), "kind": "port",
-               "sample": "one FHS iteration of the FP64 oracle on 1 channel at 1024x1024 (its full visibility "
-                         "set, 4x4 facets), scaled by 64 channels"}
+        t, sample = cpu_sample_seconds(WORKLOAD)
+        cpu = {"value": 1.0 / (t * WORKLOAD["C"]), "unit": UNIT, "cores": _ncores(), "kind": "port",
+               "sample": sample}
     if rank == 0:
         if args.precond:  # variant line: the reference's default preconditioned data term
             stage_rows["ellipse_fb_iterations_mean"] = float(np.mean([k for kl in s.ellipse_iterations() for k in kl]))

@@ -31,21 +31,6 @@ static __device__ __align__(256) double g_l2ball_partials[kScratch];
 std::mutex g_setup_mutex;
 double* g_partials_addr[64] = {nullptr};
 
-// Device address of the scratch array, resolved once per device with that
-// device current (the host-side symbol is only a stand-in).
-double* scratch_address(int device) {
-  FHS_CHECK(device >= 0 && device < 64, FHS_ERR_UNSUPPORTED, "device index >= 64");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_partials_addr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_l2ball_partials);
-    if (e != cudaSuccess)
-      throw Error(FHS_ERR_CUDA, std::string("cudaGetSymbolAddress(l2-ball scratch): ") + cudaGetErrorString(e));
-    g_partials_addr[device] = static_cast<double*>(p);
-  }
-  return g_partials_addr[device];
-}
-
 __global__ void __launch_bounds__(256) chunk_sumsq_kernel(const double* __restrict__ x, const double* __restrict__ y,
                                                           int64_t m, double* __restrict__ partials) {
   __shared__ double sh[256];
@@ -89,6 +74,31 @@ __global__ void __launch_bounds__(256) project_kernel(const double* __restrict__
   const double scale = partials[kScratch - 1];
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = y[i] + (x[i] - y[i]) * scale;
+}
+
+// Set-up, once per device with that device current: the device address of
+// the scratch array (the host-side symbol is only a stand-in for it), and
+// the three kernels' module loaded now (cudaFuncGetAttributes), so that no
+// later call loads code on the GPU -- with lazy module loading a kernel is
+// otherwise loaded at its first launch, which could fall inside a stream
+// capture.  The address is cached for the life of the process and belongs
+// to the device's primary context: after cudaDeviceReset() on that device it
+// is stale, and calls are not supported.
+double* scratch_address(int device) {
+  FHS_CHECK(device >= 0 && device < 64, FHS_ERR_UNSUPPORTED, "device index >= 64");
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!g_partials_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_l2ball_partials);
+    if (e != cudaSuccess)
+      throw Error(FHS_ERR_CUDA, std::string("cudaGetSymbolAddress(l2-ball scratch): ") + cudaGetErrorString(e));
+    cudaFuncAttributes fa;
+    FHS_CUDA(cudaFuncGetAttributes(&fa, chunk_sumsq_kernel));
+    FHS_CUDA(cudaFuncGetAttributes(&fa, scale_kernel));
+    FHS_CUDA(cudaFuncGetAttributes(&fa, project_kernel));
+    g_partials_addr[device] = static_cast<double*>(p);
+  }
+  return g_partials_addr[device];
 }
 
 }  // namespace

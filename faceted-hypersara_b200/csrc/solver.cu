@@ -718,6 +718,20 @@ fhs_status fhs_solver_iterate(fhs_solver* s_, int n, fhs_iter_info* info) {
   });
 }
 
+fhs_status fhs_solver_group_stats(fhs_solver* s_, double* out) {
+  return guarded_solver([&] {
+    Solver* S = sv(s_);
+    FHS_CHECK(S->initialised, FHS_ERR_STATE, "solver not initialised");
+    FHS_CHECK(out != nullptr, FHS_ERR_INVALID_ARG, "null output");
+    FHS_CHECK(S->iter_done >= 1, FHS_ERR_STATE, "no iteration run since fhs_solver_init");
+    DeviceGuard dg(S->op->device);
+    std::vector<double> rec;
+    read_ring(S, S->iter_done - 1, 1, rec);
+    for (int g = 0; g < S->G; ++g)
+      for (int f = 0; f < 4; ++f) out[g * 4 + f] = rec[(size_t)g * kReportFields + f];
+  });
+}
+
 fhs_status fhs_solver_update_weights(fhs_solver* s_) {
   return guarded_solver([&] {
     Solver* S = sv(s_);

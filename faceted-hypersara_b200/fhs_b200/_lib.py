@@ -115,6 +115,7 @@ SIGNATURES = {
     "fhs_solver_iterate": (C.c_int, [_vp, C.c_int, C.POINTER(IterInfo)]),
     "fhs_solver_run": (C.c_int, [_vp, C.c_int, C.POINTER(RunInfo)]),
     "fhs_solver_get_x": (C.c_int, [_vp, _dp]),
+    "fhs_solver_group_stats": (C.c_int, [_vp, _dp]),
     "fhs_solver_update_weights": (C.c_int, [_vp]),
     "fhs_solver_ellipse_iterations": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "fhs_solver_epsilon": (C.c_int, [_vp, _dp]),

@@ -546,6 +546,13 @@ class Solver:
     def update_weights(self):
         check(lib().fhs_solver_update_weights(self._h))
 
+    def group_stats(self):
+        """FP64 sums of the last iteration per spectral group, [groups, 4]:
+        sum (x - x_prev)^2, sum x^2, sum ||res_b||^2, sum eps_b^2."""
+        out = np.empty(self.G * 4)
+        check(lib().fhs_solver_group_stats(self._h, dptr(out)))
+        return out.reshape(self.G, 4)
+
     def get_state(self):
         """The solver state the reference checkpoints (facetHyperSARA.m:1071-1107):
         dict xsol/g [Ny, Nx, L], v0 (flat, per group and facet [P_q, lg]),

@@ -198,9 +198,13 @@ FHS_API fhs_status fhs_proj_l2ball(int device, int64_t n, const double* x, doubl
  * legacy default stream) and returns without synchronising.  Scratch: a
  * 512 KB static device array per device that every call shares; n is limited
  * to 134,215,680 (FHS_ERR_UNSUPPORTED above).  The first call on a device
- * resolves the array's address (cudaGetSymbolAddress), so make it before any
- * stream capture.  Calls that overlap on the GPU (other streams or devices'
- * threads racing on one device) race on the scratch: serialise them. */
+ * (n = 0 is enough) is its set-up: it resolves the array's address
+ * (cudaGetSymbolAddress) and loads the call's kernels, so make it before any
+ * stream capture.  The resolved address belongs to the device's primary
+ * context and is kept for the life of the process: after cudaDeviceReset()
+ * on that device, do not call this function again.  Calls that overlap on
+ * the GPU (other streams or devices' threads racing on one device) race on
+ * the scratch: serialise them. */
 FHS_API fhs_status fhs_proj_l2ball_noalloc(int device, int64_t n, const double* x, double eps,
                                            const double* y, double* p, void* stream);
 /* src/nuclear_norm.m:25-26  sum of singular values of x reshaped [N, L]. */
@@ -363,6 +367,13 @@ typedef enum fhs_field {
 FHS_API int64_t fhs_solver_field_size(const fhs_solver* s, int field);
 FHS_API fhs_status fhs_solver_get_field(fhs_solver* s, int field, double* out);
 FHS_API fhs_status fhs_solver_set_field(fhs_solver* s, int field, const double* in);
+/* FP64 statistics of the last iteration, per spectral group (sub-cube):
+ * out[g*4 + 0..3] = sum (x - x_prev)^2, sum x^2, sum_b ||G_b Phi x - y_b||^2,
+ * sum_b eps_b^2 over the group's channels -- the sums behind rel_val,
+ * residual and epsilon of the stopping rule (facetHyperSARA.m:877-881).
+ * A caller that splits one cube's sub-cubes over several processes sums
+ * them over the processes to take the stopping decision of the whole cube. */
+FHS_API fhs_status fhs_solver_group_stats(fhs_solver* s, double* out);
 /* Recompute reweighting weights from the current x (fhs_update_weights.m). */
 FHS_API fhs_status fhs_solver_update_weights(fhs_solver* s);
 

@@ -419,57 +419,89 @@ def adjust_noise(eps, norm_res, block_sizes, p: SolverParams):
     return out, np.array(sig)
 
 
+class FhsIteration:
+    """State of one Faceted HyperSARA sub-cube between iterations
+    (src/fhs/facetHyperSARA.m:701-889): ``step()`` runs one primal-dual
+    iteration, ``reweight()`` the weight update of :952-1137.  Initial duals
+    and weights as src/fhs/fhs_initialize_dual_and_weights.m:88-118; proj
+    starts at zero (src/fhs/fhs_initialize_data_worker.m:43)."""
+
+    def __init__(self, data: DataTerm, p: SolverParams, geom: FacetGeometry, xinit=None,
+                 precond: Precond | None = None):
+        op = data.op
+        L = data.L
+        self.data, self.p, self.geom, self.precond = data, p, geom, precond
+        self.x = np.zeros((L, op.Ny, op.Nx)) if xinit is None else np.array(xinit, dtype=np.float64)
+        tau = 0.99 / 3.0
+        self.sigma0, self.sigma1 = 1.0 / p.nu0, 1.0 / p.nu1
+        self.sigma00, self.sigma11 = tau * self.sigma0, tau * self.sigma1
+        self.sigma22 = tau / np.asarray(p.nu2, dtype=np.float64)
+        self.beta0 = np.asarray(p.gamma0, dtype=np.float64) / self.sigma0 * np.ones(geom.Q)
+        self.beta1 = p.gamma / self.sigma1
+        self.sig_bar = np.asarray(p.reweighting_sig_bar, dtype=np.float64) * np.ones(geom.Q)
+        self.facets = list(geom.facets())
+        x = self.x
+        self.v0, self.w0 = [], []
+        zero = np.linalg.norm(x) == 0
+        for q, (y0, y1), (x0, x1), win in self.facets:
+            self.v0.append(np.zeros(((y1 - y0) * (x1 - x0), L)))
+            self.w0.append(np.ones(L) if zero else
+                           nuclear_weights(win[None] * x[:, y0:y1, x0:x1], self.sig_bar[q], p.reweighting_alpha))
+        s = wv.n_coefs_sara(op.Ny, op.Nx, p.nlevel)
+        self.v1 = np.zeros((L, s))
+        self.w1 = np.ones(s) if zero else l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
+        self.v2 = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
+        self.proj = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
+        self.Fx_old = np.stack([op.A(x[l]) for l in range(L)])
+        self.g = np.zeros_like(x)
+
+    def step(self):
+        """One iteration; returns (sum (x - x_prev)^2, sum x^2, sum_b ||res_b||^2,
+        sum_b eps_b^2, norm_res per block)."""
+        x, xhat, rel_x, norm_x = primal_update(self.x, self.g)
+        self.x = x
+        self.v2, self.proj, Ftx, self.Fx_old, gres, geps, nres = _dual_step(
+            self.v2, self.proj, x, self.Fx_old, self.data, self.sigma22, self.precond)
+        gacc = np.zeros_like(x)
+        prox = pmap(lambda f: nuclear_prox_update(self.v0[f[0]], xhat[:, f[1][0]:f[1][1], f[2][0]:f[2][1]], f[3],
+                                                  self.w0[f[0]], self.beta0[f[0]]), self.facets)
+        for (q, (y0, y1), (x0, x1), win), (v0q, g0) in zip(self.facets, prox):   # overlaps summed in facet order
+            self.v0[q] = v0q
+            gacc[:, y0:y1, x0:x1] += self.sigma00 * g0
+        self.v1, g1 = l21_prox_update(self.v1, xhat, self.w1, self.beta1, self.p.nlevel)
+        self.g = gacc + self.sigma11 * g1 + Ftx
+        return rel_x, norm_x, gres, geps, nres
+
+    def reweight(self):
+        """src/fhs/fhs_update_weights.m:73-92 from the current x."""
+        x, p = self.x, self.p
+        for q, (y0, y1), (x0, x1), win in self.facets:
+            self.w0[q] = nuclear_weights(win[None] * x[:, y0:y1, x0:x1], self.sig_bar[q], p.reweighting_alpha)
+        self.w1 = l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
+
+
 def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
                     xinit=None, max_iter=None, callback=None, precond: Precond | None = None,
                     algo: str = "fhs"):
-    """src/fhs/facetHyperSARA.m:701-1138 (one spectral sub-cube); proj starts
-    at zero (src/fhs/fhs_initialize_data_worker.m:43)."""
+    """src/fhs/facetHyperSARA.m:701-1138 (one spectral sub-cube)."""
     op = data.op
     L = data.L
-    x = np.zeros((L, op.Ny, op.Nx)) if xinit is None else np.array(xinit, dtype=np.float64)
-    tau = 0.99 / 3.0
-    sigma0, sigma1 = 1.0 / p.nu0, 1.0 / p.nu1
-    sigma00, sigma11 = tau * sigma0, tau * sigma1
-    sigma22 = tau / np.asarray(p.nu2, dtype=np.float64)
-    beta0 = np.asarray(p.gamma0, dtype=np.float64) / sigma0 * np.ones(geom.Q)
-    beta1 = p.gamma / sigma1
-    sig_bar = np.asarray(p.reweighting_sig_bar, dtype=np.float64) * np.ones(geom.Q)
-    facets = list(geom.facets())
-    # fhs_initialize_dual_and_weights.m:88-118
-    v0, w0 = [], []
-    zero = np.linalg.norm(x) == 0
-    for q, (y0, y1), (x0, x1), win in facets:
-        v0.append(np.zeros(((y1 - y0) * (x1 - x0), L)))
-        w0.append(np.ones(L) if zero else
-                  nuclear_weights(win[None] * x[:, y0:y1, x0:x1], sig_bar[q], p.reweighting_alpha))
-    s = wv.n_coefs_sara(op.Ny, op.Nx, p.nlevel)
-    v1 = np.zeros((L, s))
-    w1 = np.ones(s) if zero else l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
-    v2 = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
-    proj = [[np.zeros_like(yb) for yb in data.y[l]] for l in range(L)]
-    Fx_old = np.stack([op.A(x[l]) for l in range(L)])
-    g = np.zeros_like(x)
-    log = SolverLog()
-    x_last_rw = x.copy()
-    last, rw_count = 0, 0
-    max_iter = max_iter or (p.reweighting_max_iter + 1) * p.pdfb_max_iter
     adjust = bool(p.adjust_flag_noise)
     if adjust:
-        # the l2 bounds change: work on a copy; priors off from the first
-        # iteration until the first adjustment (facetHyperSARA.m:704-708)
+        # the l2 bounds change: work on a copy
         data = DataTerm(data.op, data.G, data.y, [list(e) for e in data.eps])
-        beta0, beta1 = np.zeros(geom.Q), 0.0
+    it = FhsIteration(data, p, geom, xinit, precond)
+    log = SolverLog()
+    x_last_rw = it.x.copy()
+    last, rw_count = 0, 0
+    max_iter = max_iter or (p.reweighting_max_iter + 1) * p.pdfb_max_iter
+    if adjust:
+        # priors off from the first iteration until the first adjustment
+        # (facetHyperSARA.m:704-708)
+        it.beta0, it.beta1 = np.zeros(geom.Q), 0.0
     for t in range(1, max_iter + 1):
-        x, xhat, rel_x, norm_x = primal_update(x, g)
-        v2, proj, Ftx, Fx_old, gres, geps, nres = _dual_step(v2, proj, x, Fx_old, data, sigma22, precond)
-        gacc = np.zeros_like(x)
-        prox = pmap(lambda f: nuclear_prox_update(v0[f[0]], xhat[:, f[1][0]:f[1][1], f[2][0]:f[2][1]], f[3],
-                                                  w0[f[0]], beta0[f[0]]), facets)
-        for (q, (y0, y1), (x0, x1), win), (v0q, g0) in zip(facets, prox):   # overlaps summed in facet order
-            v0[q] = v0q
-            gacc[:, y0:y1, x0:x1] += sigma00 * g0
-        v1, g1 = l21_prox_update(v1, xhat, w1, beta1, p.nlevel)
-        g = gacc + sigma11 * g1 + Ftx
+        rel_x, norm_x, gres, geps, nres = it.step()
+        x = it.x
         rel = np.sqrt(rel_x / norm_x) if norm_x > 0 else 0.0
         res, epsn = np.sqrt(gres), np.sqrt(geps)
         log.rel_val.append(rel)
@@ -484,8 +516,8 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
             data.eps[:] = eps_new
             sig_n, sig_bar_n, *_ = compute_noise_level(op.Ny, op.Nx, L, sig_ch, algo,
                                                        geom if algo == "fhs" else None, p.nu2)
-            beta1 = p.alph * sig_n / sigma1
-            beta0 = p.alph_bar * np.asarray(sig_bar_n, dtype=np.float64) * np.ones(geom.Q) / sigma0
+            it.beta1 = p.alph * sig_n / it.sigma1
+            it.beta0 = p.alph_bar * np.asarray(sig_bar_n, dtype=np.float64) * np.ones(geom.Q) / it.sigma0
             log.n_adjust = getattr(log, "n_adjust", 0) + 1
             last = t
             continue
@@ -495,15 +527,13 @@ def facet_hypersara(data: DataTerm, p: SolverParams, geom: FacetGeometry,
             if (not p.reweighting_flag) or (rw_count >= p.reweighting_min_iter and (
                     rw_count >= p.reweighting_max_iter or rel_rw <= p.reweighting_rel_var)):
                 break
-            for q, (y0, y1), (x0, x1), win in facets:
-                w0[q] = nuclear_weights(win[None] * x[:, y0:y1, x0:x1], sig_bar[q], p.reweighting_alpha)
-            w1 = l21_weights(x, p.reweighting_sig, p.reweighting_alpha, p.nlevel)
+            it.reweight()
             x_last_rw = x.copy()
             rw_count += 1
             last = t
     log.n_reweights = rw_count
     log.epsilon_final = [list(e) for e in data.eps]
-    return x, log
+    return it.x, log
 
 
 def hypersara(data: DataTerm, p: SolverParams, xinit=None, max_iter=None, callback=None,

@@ -162,3 +162,28 @@ def test_noise_adjustment_run_matches_oracle(algo):
     for eg, eo in zip(s.epsilon(), log.epsilon_final):
         assert np.allclose(eg, eo, rtol=1e-5)
     s.close()
+
+
+def test_partitioned_driver_matches_solver_run():
+    """fhs_b200.distributed.run_partitioned over the library solver (two
+    spectral sub-cubes on this GPU, world size 1) takes the same stopping and
+    reweighting decisions as fhs_solver_run and ends on the same cube."""
+    from fhs_b200 import Solver
+    from fhs_b200 import distributed as fd
+    from fhs_b200._lib import ALGO_FHS
+    data, x, op, geom, nu2, sig, sig_bar = _setup("fhs", L=4, seed=9)
+    param = _params(nu2, [sig, sig], np.tile(sig_bar, 2), pdfb_min_iter=4, pdfb_max_iter=12,
+                    reweighting_max_iter=2)
+    kw = dict(n_groups=2, Qy=2, Qx=2, overlap=(6, 6), splits_y=[0, 30, 64], splits_x=[0, 36, 64])
+    s1 = Solver(op, ALGO_FHS, param, **kw)
+    s1.set_data(data.y, data.eps)
+    s1.init()
+    info1 = s1.run()
+    s2 = Solver(op, ALGO_FHS, param, **kw)
+    s2.set_data(data.y, data.eps)
+    s2.init()
+    info2 = fd.run_partitioned(fd.GpuSubcubes(s2, 2, 2), 2, [0, 1], param)
+    assert (info2["n_iter"], info2["n_reweights"]) == (info1["n_iter"], info1["n_reweights"])
+    assert rel(s2.x(), s1.x()) < 1e-7
+    s1.close()
+    s2.close()

@@ -46,3 +46,4 @@ def test_noalloc_rejects_oversize():
     buf = torch.zeros(2, dtype=torch.float64, device="cuda:0")
     with pytest.raises(FhsError, match="static scratch limit"):
         check(lib().fhs_proj_l2ball_noalloc(0, 1 << 40, buf.data_ptr(), 1.0, buf.data_ptr(), buf.data_ptr(), None))
+
