@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(kBuildThreads) dr_build_kernel(OpView op, int 
       if (threadIdx.x < n) {
         const float4 gm = op.geom[vo + c + threadIdx.x];
         float2 hy[7], hx[7];
-        taps<7>(op.py, gm.x, hy);
-        taps<7>(op.px, gm.y, hx);
+        taps<7>(op.py, fabsf(gm.x), hy);   // the sign bit of the stored offsets is a wrap flag
+        taps<7>(op.px, fabsf(gm.y), hx);
 #pragma unroll
         for (int a = 0; a < 7; ++a) {
           s_hy[threadIdx.x][a] = hy[a];

@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(256, 3) degrid_kernel(OpView op, const float2*
   constexpr int P = kSmemPitch;
   constexpr int R = kTileCells + J - 1;
   __shared__ float2 sm[R * P];
+  __shared__ float2 psy[R], psx[R];   // cell phases psi of the staged rows / columns
   __shared__ double bacc[kMaxBlocksPerChannel * 2];
   const WorkItem it = items[order ? order[blockIdx.x] : item0 + blockIdx.x];
   const int tile = it.tile;
@@ -79,17 +80,25 @@ __global__ void __launch_bounds__(256, 3) degrid_kernel(OpView op, const float2*
   const int a0 = t0 * kTileCells, a1 = t1 * kTileCells;
   const int Kh = op.Ky / 2 + 1;
   const float2* g = grid + (size_t)ch * (HALF ? Kh : op.Ky) * op.Kx;
+  if (threadIdx.x < R) {
+    psy[threadIdx.x] = cell_phase(wrap(a0 + threadIdx.x, op.Ky), op.Ky);
+  } else if (threadIdx.x >= 128 && threadIdx.x < 128 + R) {
+    psx[threadIdx.x - 128] = cell_phase(wrap(a1 + threadIdx.x - 128, op.Kx), op.Kx);
+  }
+  __syncthreads();
   for (int idx = threadIdx.x; idx < R * R; idx += blockDim.x) {
     const int c1 = idx / R, cc0 = idx - c1 * R;
     const int k0 = wrap(a0 + cc0, op.Ky), k1 = wrap(a1 + c1, op.Kx);
+    float2 gv;
     if (!HALF) {
-      sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * op.Ky + k0);
+      gv = __ldg(g + (size_t)k1 * op.Ky + k0);
     } else if (k0 < Kh) {
-      sm[c1 * P + cc0] = __ldg(g + (size_t)k1 * Kh + k0);
+      gv = __ldg(g + (size_t)k1 * Kh + k0);
     } else {  // Hermitian mirror
       const float2 m = __ldg(g + (size_t)(k1 == 0 ? 0 : op.Kx - k1) * Kh + (op.Ky - k0));
-      sm[c1 * P + cc0] = make_float2(m.x, -m.y);
+      gv = make_float2(m.x, -m.y);
     }
+    sm[c1 * P + cc0] = cmul(cmul(psy[cc0], psx[c1]), gv);   // psi_y psi_x G
   }
   __syncthreads();
   double nacc[NB][2];
@@ -99,9 +108,10 @@ __global__ void __launch_bounds__(256, 3) degrid_kernel(OpView op, const float2*
   // software pipeline: the next visibility's geometry and dual operands are
   // loaded while this one is interpolated
   float4 gm_n = make_float4(0.f, 0.f, 0.f, 0.f);
-  float2 yv_n = make_float2(0.f, 0.f), vv_n = yv_n, go_n = yv_n;
+  float2 yv_n = make_float2(0.f, 0.f), vv_n = yv_n, go_n = yv_n, ph_n = yv_n;
   auto fetch = [&](int i) {
     gm_n = __ldg(op.geom + vo + i);
+    ph_n = __ldg(op.vph + vo + i);
     if (DUAL) {
       yv_n = y[vo + i];
       vv_n = v2[vo + i];
@@ -111,24 +121,37 @@ __global__ void __launch_bounds__(256, 3) degrid_kernel(OpView op, const float2*
   if (beg + (int)threadIdx.x < end) fetch(beg + threadIdx.x);
   for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
     const float4 gm = gm_n;
-    const float2 yv = yv_n, vv = vv_n, go = go_n;
+    const float2 yv = yv_n, vv = vv_n, go = go_n, ph = ph_n;
     if (i + (int)blockDim.x < end) fetch(i + blockDim.x);
     const unsigned kp = __float_as_uint(gm.z);
-    const int d0 = (int)(kp & 0x3FFFu) - a0;
-    const int d1 = (int)((kp >> 14) & 0x3FFFu) - a1;
-    float2 hy[J], hx[J];
-    taps<J>(op.py, gm.x, hy);
-    taps<J>(op.px, gm.y, hx);
+    const int s0 = (int)(kp & 0x3FFFu), s1 = (int)((kp >> 14) & 0x3FFFu);
+    const int d0 = s0 - a0, d1 = s1 - a1;
+    float fy, fx;
+    int ksy, ksx;
+    axis_start(gm.x, s0, op.Ky, fy, ksy);
+    axis_start(gm.y, s1, op.Kx, fx, ksx);
+    float cy[J], cx[J];
+    rtaps<J>(op.ry, fy, cy);
+    rtaps<J>(op.rx, fx, cx);
+    tap_signs<J>(ksy, op.Ky, cy);
+    tap_signs<J>(ksx, op.Kx, cx);
+    // real taps on the phase-multiplied tile: two FMAs per tap and column
     float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
     for (int jx = 0; jx < J; ++jx) {
       const float2* col = sm + (d1 + jx) * P + d0;
-      float2 s = make_float2(0.f, 0.f);
+      float2 sc = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int jy = 0; jy < J; ++jy) s = cfma(hy[jy], col[jy], s);
-      acc = cfma(hx[jx], s, acc);
+      for (int jy = 0; jy < J; ++jy) {
+        const float2 gv = col[jy];
+        sc.x = fmaf(cy[jy], gv.x, sc.x);
+        sc.y = fmaf(cy[jy], gv.y, sc.y);
+      }
+      acc.x = fmaf(cx[jx], sc.x, acc.x);
+      acc.y = fmaf(cx[jx], sc.y, acc.y);
     }
-    const float2 gfx = make_float2(gm.w * acc.x, gm.w * acc.y);
+    const float2 pa = cmul(ph, acc);
+    const float2 gfx = make_float2(gm.w * pa.x, gm.w * pa.y);
     if (!DUAL) {
       out[vo + i] = gfx;
     } else {
@@ -179,47 +202,76 @@ __global__ void __launch_bounds__(256, 3) degrid_kernel(OpView op, const float2*
 }
 
 // ------------------------------------------------------------------ grid
-// One CTA per 64x64 grid tile and channel, 9 warps.  Warp w owns the
-// visibilities whose start column lies in band w (band 0: the 8 columns left
-// of the tile; bands 1-8: the tile's own 8-column strips), including those
-// whose start row lies in the 8 rows above the tile, and accumulates their
-// taps into a private 14-column x 64-row buffer: no atomics, no other warp
-// writes there.  Per chunk of 32 visibilities every lane evaluates the tap
-// polynomials of one visibility and stages conj(hy) and conj(hx) w v in
-// shared memory; the warp then walks the chunk one visibility at a time with
-// one lane per tap (two rounds for the 49 taps); complex accumulators with a
-// pitch of 71 (= 7 mod 32) keep each half-warp's 64-bit accesses on distinct
-// banks.  The bands are summed into the tile at the end and the tile is
-// written once.
-constexpr int kBands = kSubPerTile + 1;         // 9
-constexpr int kBandCols = kBinCells + kMaxTaps - 2;  // 14 columns covered by a band
-constexpr int kAccPitch = kTileCells + 7;       // 71
+// One CTA (8 warps) per 64x64 grid tile and channel, or per slice of a very
+// dense tile.  The tile's accumulator is FP32 complex in shared memory with
+// an even column pitch of 66 (16-byte aligned row pairs; the quarter-warp
+// accesses of a patch column fall on distinct bank groups).  Visibilities
+// that start in the tile or in the 8-cell ring above / left of it reach the
+// tile; taps that fall outside it are dropped (the neighbouring tile adds
+// them through its own ring).
+//
+// The 81 sub-bins that feed the tile (8x8 own + the ring) are processed in
+// four phases by the parity of their sub-bin row and column: two sub-bins of
+// one phase are 16 cells apart and the taps of a sub-bin's visibilities
+// cover 8 + 6 = 14 cells, so within a phase no two sub-bins touch the same
+// accumulator cell.  Warps claim the phase's sub-bins dynamically, largest
+// first (the per-item schedule is built on the host, GridPlan), and own them
+// outright: no atomics, no per-warp copies of the tile, and a fixed
+// summation order per cell (deterministic results).  Five warps per CTA fit
+// the phase sizes of a full tile (25, 20, 20, 16 sub-bins) in whole rounds.
+//
+// Inside a sub-bin the visibilities are visited grouped by 2x2 block of
+// start cells (gperm: block-major order).  All visibilities of a block touch
+// the same 8x8 patch, which the warp holds in registers (lane: column
+// lane & 7, rows 2 (lane >> 3) + {0, 1}).  The taps are phase-factored
+// (cplx.cuh): the patch accumulates real row taps sigma c_y (8 rows, zero
+// padded) times conj(phase) w v sigma c_x (8 columns), two real-by-complex
+// FMAs per lane and visibility; the cell phases conj(psi_y psi_x) are
+// applied once per cell when the tile is written.  A patch is added into the
+// shared accumulator once per block, and the tile is written once.
+constexpr int kGPitch = kTileCells + 2;             // 66
+constexpr int kGWarps = 5;
+constexpr int kGStage = 28;                         // floats per staged visibility: 8 a + 8 complex b + 4 pad
+constexpr int kGSub = (kSubPerTile + 1) * (kSubPerTile + 1);  // 81 sub-bins feed a tile
 
-struct BandRange {
-  int beg, end;
-  int ring0;  // start rows above the tile (wrap-adjusted offsets)
-};
+// adds a lane's two patch cells (rows row, row + 1 of column col, tile
+// coordinates) into the accumulator; cells outside the tile are dropped
+static __device__ __forceinline__ void patch_flush(float2* acc, int row, int col, float2 p0, float2 p1) {
+  if (row >= 0 && row < kTileCells && col >= 0 && col < kTileCells) {
+    float4* cell = reinterpret_cast<float4*>(acc + col * kGPitch + row);
+    float4 c = *cell;
+    c.x += p0.x;
+    c.y += p0.y;
+    c.z += p1.x;
+    c.w += p1.y;
+    *cell = c;
+  }
+}
 
 // MODE 0: gridB = G^H vin.  MODE 1: l2-ball dual, pass 2 (v2 = z scale).
 // MODE 2: ellipsoid dual, pass 2 (v2 = pU (d - w), w = proj - y).
 template <int J, int MODE>
-__global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __restrict__ gridB,
-                                                           const WorkItem* __restrict__ items,
-                                                           const int* __restrict__ order, int item0,
-                                                           float2* __restrict__ partial,
-                                                           const float2* __restrict__ vin,
-                                                           float2* __restrict__ v2,
-                                                           const float* __restrict__ blk_scale,
-                                                           const float2* __restrict__ zbuf, PrecondView pc) {
+__global__ void __launch_bounds__(kGWarps * 32, 4) grid_kernel(OpView op, float2* __restrict__ gridB,
+                                                               const WorkItem* __restrict__ items,
+                                                               const int* __restrict__ order, int item0,
+                                                               float2* __restrict__ partial,
+                                                               const float2* __restrict__ vin,
+                                                               float2* __restrict__ v2,
+                                                               const float* __restrict__ blk_scale,
+                                                               const float2* __restrict__ zbuf, PrecondView pc,
+                                                               const int32_t* __restrict__ gperm,
+                                                               const GridPlan* __restrict__ plans) {
+  static_assert(J == 7, "the 8x8 patch of a 2x2 start block holds 7 taps per axis");
   constexpr bool DUAL = MODE != 0;
-  static_assert(J <= kMaxTaps && J * J <= 64, "two tap rounds per visibility");
-  extern __shared__ float2 gsm2[];
-  float2* acc = gsm2;                                           // [kBands][kBandCols][kAccPitch]
-  float2* stage = acc + kBands * kBandCols * kAccPitch;         // [kBands][32][2J]
-  int2* stage_d = reinterpret_cast<int2*>(stage + kBands * 32 * 2 * J);  // [kBands][32]
-  __shared__ BandRange rng[kBands][2];
-  __shared__ int any;
-  const WorkItem it = items[order ? order[blockIdx.x] : item0 + blockIdx.x];
+  extern __shared__ float4 gsm4[];
+  float2* acc = reinterpret_cast<float2*>(gsm4);                 // [kTileCells cols][kGPitch]
+  float* stage_all = reinterpret_cast<float*>(acc + kTileCells * kGPitch);   // [warps][32][kGStage]
+  __shared__ float2 psy[kTileCells], psx[kTileCells];             // cell phases of the tile's rows / columns
+  __shared__ int2 rng[kGSub];
+  __shared__ GridPlan plan;
+  __shared__ int pclaim[4];
+  const int itx = order ? order[blockIdx.x] : item0 + blockIdx.x;
+  const WorkItem it = items[itx];
   const int tile = it.tile;
   const int ch = it.ch;
   const int t0 = tile % op.nT0, t1 = tile / op.nT0;
@@ -227,49 +279,37 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
   const int T0 = min(kTileCells, op.Ky - a0), T1 = min(kTileCells, op.Kx - a1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t* off = op.sb_off + (size_t)ch * (op.nkeys + 1);
-  if (threadIdx.x == 0) any = 0;
-  __syncthreads();
-  if (lane == 0) {
-    // band 0 = the sub-bin column left of the tile (wraps), bands 1-8 = the tile's columns
-    const int sbr0 = (t0 * kSubPerTile - 1 + op.nsb0) % op.nsb0;  // sub-bin row above the tile
+  if (threadIdx.x < (int)(sizeof(GridPlan) / 4))
+    reinterpret_cast<int*>(&plan)[threadIdx.x] = reinterpret_cast<const int*>(plans + itx)[threadIdx.x];
+  if (threadIdx.x < 4) pclaim[threadIdx.x] = 0;
+  if (threadIdx.x >= 32 && threadIdx.x < 32 + kTileCells) {
+    const int r = threadIdx.x - 32;
+    psy[r] = cell_phase(wrap(a0 + r, op.Ky), op.Ky);
+    psx[r] = cell_phase(wrap(a1 + r, op.Kx), op.Kx);
+  }
+  // ---- the 81 sub-bins: (i, j) in [-1, 8)^2, -1 = the ring (wraps)
+  if (threadIdx.x >= 64 && threadIdx.x < 64 + kGSub) {
+    const int t = threadIdx.x - 64;
+    const int i = t % (kSubPerTile + 1) - 1, j = t / (kSubPerTile + 1) - 1;
     const int nrows = min(kSubPerTile, op.nsb0 - t0 * kSubPerTile);
-    int sb1;
-    bool ok = true;
-    if (warp == 0) {
-      sb1 = (t1 * kSubPerTile - 1 + op.nsb1) % op.nsb1;
-    } else {
-      sb1 = t1 * kSubPerTile + warp - 1;
-      ok = sb1 < op.nsb1;
+    const int ncols = min(kSubPerTile, op.nsb1 - t1 * kSubPerTile);
+    int2 r = make_int2(0, 0);
+    if (i < nrows && j < ncols) {
+      const int sb0 = i < 0 ? (t0 * kSubPerTile - 1 + op.nsb0) % op.nsb0 : t0 * kSubPerTile + i;
+      const int sb1 = j < 0 ? (t1 * kSubPerTile - 1 + op.nsb1) % op.nsb1 : t1 * kSubPerTile + j;
+      const int key = ((sb1 / kSubPerTile) * op.nT0 + sb0 / kSubPerTile) * (kSubPerTile * kSubPerTile) +
+                      (sb1 % kSubPerTile) * kSubPerTile + (sb0 % kSubPerTile);
+      const int b = off[key], e = off[key + 1];
+      const int len = e - b;
+      r.x = b + (int)(((int64_t)len * it.split) / it.nsplit);
+      r.y = b + (int)(((int64_t)len * (it.split + 1)) / it.nsplit);
     }
-    BandRange r0{0, 0, 0}, r1{0, 0, 1};
-    if (ok) {
-      const int base =
-          ((sb1 / kSubPerTile) * op.nT0 + t0) * (kSubPerTile * kSubPerTile) + (sb1 % kSubPerTile) * kSubPerTile;
-      r0.beg = off[base];
-      r0.end = off[base + nrows];
-      const int kr = ((sb1 / kSubPerTile) * op.nT0 + sbr0 / kSubPerTile) * (kSubPerTile * kSubPerTile) +
-                     (sb1 % kSubPerTile) * kSubPerTile + (sbr0 % kSubPerTile);
-      r1.beg = off[kr];
-      r1.end = off[kr + 1];
-    }
-    // this item's slice of both ranges
-    auto slice = [&](BandRange r) {
-      const int len = r.end - r.beg;
-      BandRange q = r;
-      q.beg = r.beg + (int)(((int64_t)len * it.split) / it.nsplit);
-      q.end = r.beg + (int)(((int64_t)len * (it.split + 1)) / it.nsplit);
-      return q;
-    };
-    r0 = slice(r0);
-    r1 = slice(r1);
-    rng[warp][0] = r0;
-    rng[warp][1] = r1;
-    if (r0.end > r0.beg || r1.end > r1.beg) atomicOr(&any, 1);
+    rng[t] = r;
   }
   __syncthreads();
   // split tiles write a partial tile (summed by grid_combine_kernel)
   float2* gb;
-  size_t ld;  // leading dimension of the destination
+  size_t ld;
   int g0, g1;
   if (it.slot >= 0) {
     gb = partial + (size_t)it.slot * kTileCells * kTileCells;
@@ -282,108 +322,139 @@ __global__ void __launch_bounds__(kBands * 32) grid_kernel(OpView op, float2* __
     g0 = a0;
     g1 = a1;
   }
-  if (!any) {
+  const int nsub = plan.count[0] + plan.count[1] + plan.count[2] + plan.count[3];
+  if (nsub == 0) {   // nothing reaches the tile: zeros
     for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
       const int cc1 = idx / T0, cc0 = idx - cc1 * T0;
       gb[(size_t)(g1 + cc1) * ld + g0 + cc0] = make_float2(0.f, 0.f);
     }
     return;
   }
-  for (int i = threadIdx.x; i < kBands * kBandCols * kAccPitch; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+  for (int k = threadIdx.x; k < kTileCells * kGPitch / 2; k += blockDim.x) gsm4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
   const int64_t vo = op.ch_voff[ch];
   const float* scl = DUAL ? blk_scale + (size_t)ch * kMaxBlocksPerChannel : nullptr;
-  const int xb = warp == 0 ? -kBinCells : (warp - 1) * kBinCells;  // first tile column of the band buffer
-  float2* ab = acc + warp * kBandCols * kAccPitch;
-  float2* st = stage + warp * 32 * 2 * J;
-  int2* sd = stage_d + warp * 32;
-  // per-lane tap constants of the two rounds
-  int jyA, jxA, jyB, jxB;
-  {
-    const int tA = lane, tB = lane + 32;
-    jxA = tA / J;
-    jyA = tA - jxA * J;
-    jxB = tB / J;
-    jyB = tB - jxB * J;
-  }
-  const bool hasB = lane + 32 < J * J;
-  const int offA = jxA * kAccPitch + jyA, offB = jxB * kAccPitch + jyB;
-  for (int part = 0; part < 2; ++part) {
-    const BandRange r = rng[warp][part];
-    for (int base = r.beg; base < r.end; base += 32) {
-      const int n = min(32, r.end - base);
-      if (lane < n) {
-        const int i = base + lane;
-        const float4 gm = __ldg(op.geom + vo + i);
-        const unsigned kp = __float_as_uint(gm.z);
-        int d0 = (int)(kp & 0x3FFFu) - a0;
-        int d1 = (int)((kp >> 14) & 0x3FFFu) - a1;
-        if (r.ring0 && d0 >= 0) d0 -= op.Ky;
-        if (warp == 0 && d1 >= 0) d1 -= op.Kx;
-        float2 v;
-        if (MODE == 1) {
-          const float2 z = zbuf[vo + i];
-          const float sc = scl[kp >> 28];
-          v = make_float2(z.x * sc, z.y * sc);
-          if (part == 0 && warp > 0) v2[vo + i] = v;  // the owner tile writes the dual
-        } else if (MODE == 2) {
-          const float2 d = zbuf[vo + i];
-          const double2 w = pc.w[vo + i];
-          const double p = (double)pc.pu[vo + i];
-          v = make_float2((float)(p * ((double)d.x - w.x)), (float)(p * ((double)d.y - w.y)));
-          if (part == 0 && warp > 0) v2[vo + i] = v;
-        } else {
-          v = vin[vo + i];
-        }
-        v.x *= gm.w;
-        v.y *= gm.w;
-        float2 hy[J], hx[J];
-        taps<J>(op.py, gm.x, hy);
-        taps<J>(op.px, gm.y, hx);
+  float* st = stage_all + warp * 32 * kGStage;
+  const int pc_col = lane & 7, pc_rp = lane >> 3;   // this lane's patch column and row pair
+  const float2* sa = reinterpret_cast<const float2*>(st + 2 * pc_rp);      // staged row taps of its two rows
+  const float2* sbp = reinterpret_cast<const float2*>(st + 8 + 2 * pc_col);  // staged column value
+  constexpr int kSt2 = kGStage / 2;                                         // float2 per staged visibility
+  int pbase = 0;
+  for (int ph = 0; ph < 4; ++ph) {
+    const int nph = plan.count[ph];
+    for (;;) {
+      int idx = 0;
+      if (lane == 0) idx = atomicAdd(&pclaim[ph], 1);
+      idx = __shfl_sync(0xffffffffu, idx, 0);
+      if (idx >= nph) break;
+      const int sb = plan.sub[pbase + idx];
+      const int2 r = rng[sb];
+      const int i = sb % (kSubPerTile + 1) - 1, j = sb / (kSubPerTile + 1) - 1;
+      const bool own = i >= 0 && j >= 0;
+      const int rowb = kBinCells * i + 2 * pc_rp, colb = kBinCells * j + pc_col;   // tile coordinates
+      float2 p0 = make_float2(0.f, 0.f), p1 = p0;   // this lane's two patch cells
+      int cur = -1;                                  // 2x2 start block held in p0/p1
+      for (int base = r.x; base < r.y; base += 32) {
+        const int n = min(32, r.y - base);
+        int blk = 16;
+        if (lane < n) {
+          const int q = gperm[vo + base + lane];      // channel-relative storage index
+          const float4 gm = __ldg(op.geom + vo + q);
+          const unsigned kp = __float_as_uint(gm.z);
+          const int s0 = (int)(kp & 0x3FFFu), s1 = (int)((kp >> 14) & 0x3FFFu);
+          float2 v;
+          if (MODE == 1) {
+            const float2 z = zbuf[vo + q];
+            const float sc = scl[kp >> 28];
+            v = make_float2(z.x * sc, z.y * sc);
+            if (own) v2[vo + q] = v;   // the owner tile writes the dual
+          } else if (MODE == 2) {
+            const float2 d = zbuf[vo + q];
+            const double2 w = pc.w[vo + q];
+            const double pu = (double)pc.pu[vo + q];
+            v = make_float2((float)(pu * ((double)d.x - w.x)), (float)(pu * ((double)d.y - w.y)));
+            if (own) v2[vo + q] = v;
+          } else {
+            v = vin[vo + q];
+          }
+          float fy, fx;
+          int ksy, ksx;
+          axis_start(gm.x, s0, op.Ky, fy, ksy);
+          axis_start(gm.y, s1, op.Kx, fx, ksx);
+          float cy[J], cx[J];
+          rtaps<J>(op.ry, fy, cy);
+          rtaps<J>(op.rx, fx, cx);
+          tap_signs<J>(ksy, op.Ky, cy);
+          tap_signs<J>(ksx, op.Kx, cx);
+          v = cmulc(__ldg(op.vph + vo + q), make_float2(v.x * gm.w, v.y * gm.w));   // conj(phase) w v
+          // zero-padded 8-tap rows / columns of the 2x2 block's patch
+          const bool dy = s0 & 1, dx = s1 & 1;
+          float ap[8], bp[8];
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-          st[lane * 2 * J + j] = make_float2(hy[j].x, -hy[j].y);   // conj(hy)
-          st[lane * 2 * J + J + j] = cmulc(hx[j], v);               // conj(hx) w v
+          for (int t = 0; t < 8; ++t) {
+            ap[t] = dy ? (t > 0 ? cy[t - 1] : 0.f) : (t < J ? cy[t] : 0.f);
+            bp[t] = dx ? (t > 0 ? cx[t - 1] : 0.f) : (t < J ? cx[t] : 0.f);
+          }
+          float4* sl = reinterpret_cast<float4*>(st + lane * kGStage);
+          sl[0] = make_float4(ap[0], ap[1], ap[2], ap[3]);
+          sl[1] = make_float4(ap[4], ap[5], ap[6], ap[7]);
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+            sl[2 + t] = make_float4(bp[2 * t] * v.x, bp[2 * t] * v.y, bp[2 * t + 1] * v.x, bp[2 * t + 1] * v.y);
+          blk = ((s0 & 7) >> 1) | (((s1 & 7) >> 1) << 2);
         }
-        sd[lane] = make_int2((d1 - xb) * kAccPitch + d0, d0);
+        int prev = __shfl_up_sync(0xffffffffu, blk, 1);
+        if (lane == 0) prev = cur;
+        const unsigned change = __ballot_sync(0xffffffffu, lane < n && blk != prev);
+        __syncwarp();
+        int k = 0;
+        while (k < n) {   // runs of one 2x2 block (warp-uniform bounds)
+          if ((change >> k) & 1u) {
+            if (cur >= 0) patch_flush(acc, rowb + 2 * (cur & 3), colb + 2 * (cur >> 2), p0, p1);
+            cur = __shfl_sync(0xffffffffu, blk, k);
+            p0 = make_float2(0.f, 0.f);
+            p1 = p0;
+          }
+          const unsigned rest = change & ~((2u << k) - 1u);
+          const int kend = rest ? __ffs(rest) - 1 : n;
+          for (; k + 2 <= kend; k += 2) {
+            const float2 a = sa[k * kSt2], b = sbp[k * kSt2];
+            const float2 a2 = sa[(k + 1) * kSt2], b2 = sbp[(k + 1) * kSt2];
+            p0.x = fmaf(a.x, b.x, p0.x);
+            p0.y = fmaf(a.x, b.y, p0.y);
+            p1.x = fmaf(a.y, b.x, p1.x);
+            p1.y = fmaf(a.y, b.y, p1.y);
+            p0.x = fmaf(a2.x, b2.x, p0.x);
+            p0.y = fmaf(a2.x, b2.y, p0.y);
+            p1.x = fmaf(a2.y, b2.x, p1.x);
+            p1.y = fmaf(a2.y, b2.y, p1.y);
+          }
+          if (k < kend) {
+            const float2 a = sa[k * kSt2], b = sbp[k * kSt2];
+            p0.x = fmaf(a.x, b.x, p0.x);
+            p0.y = fmaf(a.x, b.y, p0.y);
+            p1.x = fmaf(a.y, b.x, p1.x);
+            p1.y = fmaf(a.y, b.y, p1.y);
+            ++k;
+          }
+        }
+        __syncwarp();   // the stage is rewritten by the next chunk
       }
-      __syncwarp();
-      // Taps outside the tile need no test: columns left of the tile (band 0)
-      // or right of it (band 8, columns 8-13) land in band columns the final
-      // sum ignores, and own rows stay below 64 + 7 <= kAccPitch.  Only the
-      // ring above the tile (part 1) reaches negative rows, which are skipped.
-      if (part == 0) {
-        for (int k = 0; k < n; ++k) {
-          const int a = sd[k].x;                // accumulator index of tap (0, 0)
-          const float2* sk = st + k * 2 * J;
-          ab[a + offA] = cfma(sk[jyA], sk[J + jxA], ab[a + offA]);
-          if (hasB) ab[a + offB] = cfma(sk[jyB], sk[J + jxB], ab[a + offB]);
-          __syncwarp();
-        }
-      } else {
-        for (int k = 0; k < n; ++k) {
-          const int2 d = sd[k];                 // (accumulator index, row offset)
-          const float2* sk = st + k * 2 * J;
-          if (d.y + jyA >= 0) ab[d.x + offA] = cfma(sk[jyA], sk[J + jxA], ab[d.x + offA]);
-          if (hasB && d.y + jyB >= 0) ab[d.x + offB] = cfma(sk[jyB], sk[J + jxB], ab[d.x + offB]);
-          __syncwarp();
-        }
-      }
+      if (cur >= 0) patch_flush(acc, rowb + 2 * (cur & 3), colb + 2 * (cur >> 2), p0, p1);
     }
+    pbase += nph;
+    __syncthreads();   // the next phase's sub-bins overlap this phase's patches
   }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
-    const int c = idx / T0, rr = idx - c * T0;
-    const int w1 = c / kBinCells + 1;      // band whose own strip holds column c
-    float2 val = acc[w1 * kBandCols * kAccPitch + (c - (w1 - 1) * kBinCells) * kAccPitch + rr];
-    const int w0 = w1 - 1;                 // the band to the left reaches 6 columns into the strip
-    const int cl = c - (w0 == 0 ? -kBinCells : (w0 - 1) * kBinCells);
-    if (cl < kBandCols) {
-      const float2 o = acc[w0 * kBandCols * kAccPitch + cl * kAccPitch + rr];
-      val.x += o.x;
-      val.y += o.y;
+  if (T0 == kTileCells) {
+    for (int idx = threadIdx.x; idx < kTileCells * T1; idx += blockDim.x) {
+      const int c = idx >> 6, rr = idx & (kTileCells - 1);
+      gb[(size_t)(g1 + c) * ld + g0 + rr] = cmulc(cmul(psy[rr], psx[c]), acc[c * kGPitch + rr]);  // conj(psi) acc
     }
-    gb[(size_t)(g1 + c) * ld + g0 + rr] = val;
+  } else {
+    for (int idx = threadIdx.x; idx < T0 * T1; idx += blockDim.x) {
+      const int c = idx / T0, rr = idx - c * T0;
+      gb[(size_t)(g1 + c) * ld + g0 + rr] = cmulc(cmul(psy[rr], psx[c]), acc[c * kGPitch + rr]);
+    }
   }
 }
 
@@ -408,8 +479,8 @@ __global__ void __launch_bounds__(256) grid_combine_kernel(OpView op, float2* __
   }
 }
 
-constexpr size_t kGridSmem = kBands * kBandCols * kAccPitch * sizeof(float2) +
-                             kBands * 32 * 2 * kMaxTaps * sizeof(float2) + kBands * 32 * sizeof(int2);
+constexpr size_t kGridSmem = (size_t)kTileCells * kGPitch * sizeof(float2) +
+                             (size_t)kGWarps * 32 * kGStage * sizeof(float);
 
 template <int J, int MODE>
 void launch_grid_kernel(const MeasOp* op, int c0, int nc, const float2* vin, float2* v2, const float* scale,
@@ -424,9 +495,13 @@ void launch_grid_kernel(const MeasOp* op, int c0, int nc, const float2* vin, flo
   }
   const int i0 = op->h_gr_off[c0], n = op->h_gr_off[c0 + nc] - i0;
   if (n > 0) {
-    grid_kernel<J, MODE><<<n, kBands * 32, kGridSmem, s>>>(op->view(), op->gridB.p, op->gr_items.p,
-                                                           nullptr, i0, op->gr_partial.p,
-                                                           vin, v2, scale, zbuf, pc);
+    // the whole operator at once: items largest first (gr_order), so the
+    // densest tiles do not end up in the tail of the launch
+    const bool all = c0 == 0 && nc == op->L;
+    grid_kernel<J, MODE><<<n, kGWarps * 32, kGridSmem, s>>>(op->view(), op->gridB.p, op->gr_items.p,
+                                                            all ? op->gr_order.p : nullptr, i0,
+                                                            op->gr_partial.p, vin, v2, scale, zbuf, pc,
+                                                            op->gperm.p, op->gr_plan.p);
     count_launch();
     FHS_LAUNCH_CHECK();
   }
@@ -532,6 +607,11 @@ OpView MeasOp::view() const {
         v.py[j][part][k] = j < Jy ? (float)ay.poly[((size_t)j * 2 + part) * nt + k] : 0.f;
         v.px[j][part][k] = j < Jx ? (float)ax.poly[((size_t)j * 2 + part) * nt + k] : 0.f;
       }
+  for (int j = 0; j < kMaxTaps; ++j)
+    for (int k = 0; k < nt; ++k) {
+      v.ry[j][k] = j < Jy ? (float)ay.poly_real[(size_t)j * nt + k] : 0.f;
+      v.rx[j][k] = j < Jx ? (float)ax.poly_real[(size_t)j * nt + k] : 0.f;
+    }
   v.Ny = Ny;
   v.Nx = Nx;
   v.Ky = Ky;
@@ -548,6 +628,7 @@ OpView MeasOp::view() const {
   v.sy = sy.p;
   v.sx = sx.p;
   v.geom = geom.p;
+  v.vph = vph.p;
   v.sb_off = sb_off.p;
   v.ch_voff = ch_voff.p;
   v.ch_M = ch_M.p;
@@ -633,8 +714,11 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
   for (int64_t m = 0; m < n; ++m) {
     while (m >= blk_end) blk_end += block_sizes[++blk];
     FHS_CHECK(std::isfinite(om_y[m]) && std::isfinite(om_x[m]), FHS_ERR_NUMERIC, "non-finite frequency");
-    const double uy = om_y[m] / gy - op->Jy / 2.0;
-    const double ux = om_x[m] / gx - op->Jx / 2.0;
+    // frequencies are 2 pi periodic (integer pixel positions): take them in [-pi, pi)
+    const double oyn = om_y[m] - 2.0 * M_PI * std::floor((om_y[m] + M_PI) / (2.0 * M_PI));
+    const double oxn = om_x[m] - 2.0 * M_PI * std::floor((om_x[m] + M_PI) / (2.0 * M_PI));
+    const double uy = oyn / gy - op->Jy / 2.0;
+    const double ux = oxn / gx - op->Jx / 2.0;
     const double fy0 = std::floor(uy), fx0 = std::floor(ux);
     float fy = (float)(uy - fy0), fx = (float)(ux - fx0);
     if (fy >= 1.f) fy = std::nextafter(1.f, 0.f);
@@ -647,6 +731,10 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
     const float wt = w ? (float)w[m] : 1.f;
     float kpf;
     std::memcpy(&kpf, &kp, sizeof(kpf));
+    // the sign bit of the fractional offsets marks a negative unwrapped
+    // first tap k0 + 1 (the kernels resolve the grid wrap with it)
+    if (fy0 + 1 < 0) fy = std::copysign(fy, -1.f);
+    if (fx0 + 1 < 0) fx = std::copysign(fx, -1.f);
     g[m] = make_float4(fy, fx, kpf, wt);
     const int sb0 = (int)s0 / kBinCells, sb1 = (int)s1 / kBinCells;
     key[m] = ((sb1 / kSubPerTile) * op->nT0 + sb0 / kSubPerTile) * (kSubPerTile * kSubPerTile) +
@@ -690,6 +778,33 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
       h.perm[a + i] = tp[idx[i]];
     }
   }
+  // per-visibility tap phase exp(i (om_y + om_x) / 2) of the frequencies
+  // taken in [-pi, pi), in sorted order (FP64 on the host)
+  h.vph.resize(n);
+  for (int64_t p = 0; p < n; ++p) {
+    const int64_t m = h.perm[p];
+    const double oyn = om_y[m] - 2.0 * M_PI * std::floor((om_y[m] + M_PI) / (2.0 * M_PI));
+    const double oxn = om_x[m] - 2.0 * M_PI * std::floor((om_x[m] + M_PI) / (2.0 * M_PI));
+    const double ph = 0.5 * (oyn + oxn);
+    h.vph[p] = make_float2((float)std::cos(ph), (float)std::sin(ph));
+  }
+  // Gridding order: inside each sub-bin, the visibilities grouped by 2x2
+  // block of start cells (block-major, stable), as positions in the sorted
+  // order above; the gridding kernel accumulates one block's 8x8 patch in
+  // registers.
+  h.gperm.resize(n);
+  for (int k = 0; k < op->nkeys; ++k) {
+    const int a = h.sb_off[k], b = h.sb_off[k + 1];
+    int cnt[17] = {0};
+    auto block_of = [&](int i) {
+      unsigned kp;
+      std::memcpy(&kp, &h.geom[i].z, sizeof(kp));
+      return (int)(((kp & 7u) >> 1) | ((((kp >> 14) & 7u) >> 1) << 2));
+    };
+    for (int i = a; i < b; ++i) cnt[block_of(i) + 1]++;
+    for (int t = 0; t < 16; ++t) cnt[t + 1] += cnt[t];
+    for (int i = a; i < b; ++i) h.gperm[a + cnt[block_of(i)]++] = i;
+  }
   h.set = true;
 }
 
@@ -701,7 +816,7 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
 // gridding output is zeroed at commit).  Items run channel by channel in tile
 // order, so neighbouring tiles (which share aprons) run close together.
 constexpr int kDegridSlice = 8192;
-constexpr int kGridSlice = 4096;
+constexpr int kGridSlice = 32768;
 
 static void build_work_lists(MeasOp* op, cudaStream_t s) {
   const int L = op->L, nt = op->ntiles();
@@ -710,6 +825,8 @@ static void build_work_lists(MeasOp* op, cudaStream_t s) {
     return ((sb1 / S) * op->nT0 + sb0 / S) * (S * S) + (sb1 % S) * S + (sb0 % S);
   };
   std::vector<WorkItem> dg, gr;
+  std::vector<int> gr_work;   // visibilities an item grids (own + ring)
+  std::vector<GridPlan> plans;
   std::vector<GridCombine> comb;
   op->h_dg_off.assign(L + 1, 0);
   op->h_gr_off.assign(L + 1, 0);
@@ -735,13 +852,37 @@ static void build_work_lists(MeasOp* op, cudaStream_t s) {
       ring += off[key(sbr0, sbc1) + 1] - off[key(sbr0, sbc1)];
       const int tot = own + ring;
       if (tot == 0) continue;
+      // sub-bin schedule: phases by parity, largest first (ties by index)
+      GridPlan plan{};
+      {
+        const int nrows = std::min(S, op->nsb0 - t0 * S), ncols = std::min(S, op->nsb1 - t1 * S);
+        std::vector<std::pair<int, int>> ph[4];   // (-size, sub-bin index)
+        for (int j = -1; j < S; ++j)
+          for (int i = -1; i < S; ++i) {
+            if (i >= nrows || j >= ncols) continue;
+            const int sb0 = i < 0 ? sbr0 : t0 * S + i, sb1 = j < 0 ? sbc1 : t1 * S + j;
+            const int len = off[key(sb0, sb1) + 1] - off[key(sb0, sb1)];
+            if (len == 0) continue;
+            ph[((i + 1) & 1) | (((j + 1) & 1) << 1)].push_back({-len, (j + 1) * (S + 1) + (i + 1)});
+          }
+        int pos = 0;
+        for (int q = 0; q < 4; ++q) {
+          std::sort(ph[q].begin(), ph[q].end());
+          plan.count[q] = (int)ph[q].size();
+          for (const auto& e : ph[q]) plan.sub[pos++] = (uint8_t)e.second;
+        }
+      }
       const int ns = (tot + kGridSlice - 1) / kGridSlice;
       if (ns == 1) {
         gr.push_back(WorkItem{c, t, 0, 1, -1, 0});
+        gr_work.push_back(tot);
+        plans.push_back(plan);
       } else {
         comb.push_back(GridCombine{c, t, pslot, ns});
         for (int k = 0; k < ns; ++k) {
           gr.push_back(WorkItem{c, t, k, ns, pslot + k, 0});
+          gr_work.push_back(tot / ns);
+          plans.push_back(plan);
         }
         pslot += ns;
       }
@@ -754,6 +895,16 @@ static void build_work_lists(MeasOp* op, cudaStream_t s) {
   op->dg_items.upload(dg.data(), dg.size(), s);
   op->gr_items.alloc(std::max<size_t>(gr.size(), 1));
   op->gr_items.upload(gr.data(), gr.size(), s);
+  // launch order of the whole-operator gridding: largest item first (ties:
+  // item order), so the long dense tiles start at once and the short ones
+  // fill in behind them
+  std::vector<int> gord(gr.size());
+  for (size_t k = 0; k < gord.size(); ++k) gord[k] = (int)k;
+  std::stable_sort(gord.begin(), gord.end(), [&](int u, int v) { return gr_work[u] > gr_work[v]; });
+  op->gr_order.alloc(std::max<size_t>(gord.size(), 1));
+  op->gr_order.upload(gord.data(), gord.size(), s);
+  op->gr_plan.alloc(std::max<size_t>(plans.size(), 1));
+  op->gr_plan.upload(plans.data(), plans.size(), s);
   op->gr_combine.alloc(std::max<size_t>(comb.size(), 1));
   op->gr_combine.upload(comb.data(), comb.size(), s);
   op->dg_off.alloc(L + 1);
@@ -807,12 +958,21 @@ void measop_commit(MeasOp* op) {
   }
   op->zbuf.alloc(std::max<int64_t>(op->Mtot, 1));
   op->perm.alloc(std::max<int64_t>(op->Mtot, 1));
+  if (!op->dr) {
+    op->gperm.alloc(std::max<int64_t>(op->Mtot, 1));
+    op->vph.alloc(std::max<int64_t>(op->Mtot, 1));
+  }
   for (int c = 0; c < L; ++c) {
     const ChannelHost& h = op->ch[c];
     if (h.M) {
-      if (!op->dr)
+      if (!op->dr) {
         FHS_CUDA(cudaMemcpyAsync(op->geom.p + op->h_voff[c], h.geom.data(), h.M * sizeof(float4),
                                  cudaMemcpyHostToDevice, s));
+        FHS_CUDA(cudaMemcpyAsync(op->gperm.p + op->h_voff[c], h.gperm.data(), h.M * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, s));
+        FHS_CUDA(cudaMemcpyAsync(op->vph.p + op->h_voff[c], h.vph.data(), h.M * sizeof(float2),
+                                 cudaMemcpyHostToDevice, s));
+      }
       FHS_CUDA(cudaMemcpyAsync(op->perm.p + op->h_voff[c], h.perm.data(), h.M * sizeof(int32_t),
                                cudaMemcpyHostToDevice, s));
     }
@@ -853,6 +1013,8 @@ void measop_commit(MeasOp* op) {
   for (auto& h : op->ch) {
     std::vector<float4>().swap(h.geom);
     std::vector<int32_t>().swap(h.perm);
+    std::vector<int32_t>().swap(h.gperm);
+    std::vector<float2>().swap(h.vph);
   }
   op->committed = true;
 }

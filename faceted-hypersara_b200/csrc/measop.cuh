@@ -13,6 +13,9 @@ struct OpView {
   // tap polynomials (kernel parameters: uniform across threads)
   float py[kMaxTaps][2][kPolyDegree + 1];
   float px[kMaxTaps][2][kPolyDegree + 1];
+  // the real taps c_j of the phase-factored form (see cplx.cuh)
+  float ry[kMaxTaps][kPolyDegree + 1];
+  float rx[kMaxTaps][kPolyDegree + 1];
   int Ny, Nx, Ky, Kx, Jy, Jx;
   int nT0, nT1;      // tiles per axis (kTileCells cells each, last may be partial)
   int nsb0, nsb1;    // sub-bins per axis (kBinCells cells each)
@@ -22,6 +25,7 @@ struct OpView {
   const float* sy;      // [Ny] scaling factors
   const float* sx;      // [Nx]
   const float4* geom;   // per sorted visibility: (fy, fx, kpack bits, weight)
+  const float2* vph;    // per sorted visibility: exp(i (om_y + om_x) / 2), the tap phase of the visibility
   const int32_t* sb_off;  // [L][nkeys+1] visibility offsets per sub-bin (channel-relative)
   const int64_t* ch_voff; // [L] first visibility of each channel
   const int32_t* ch_M;    // [L]
@@ -49,6 +53,15 @@ struct FbItem {
   int ch, beg, end, pad;
 };
 
+// Sub-bin schedule of one gridding item: the non-empty sub-bins that reach
+// the tile (index (j + 1) * 9 + (i + 1) for sub-bin row i, column j in
+// [-1, 8), -1 = the ring), grouped by phase (parity of i + 1, j + 1) and
+// largest first within a phase.
+struct GridPlan {
+  int count[4];      // sub-bins per phase
+  uint8_t sub[84];   // phase 0 entries, then phase 1, ...
+};
+
 struct GridCombine {
   int ch, tile, pbase, nsplit;
 };
@@ -56,6 +69,8 @@ struct GridCombine {
 struct ChannelHost {
   std::vector<float4> geom;        // sorted order
   std::vector<int32_t> perm;       // sorted position -> original index
+  std::vector<int32_t> gperm;      // gridding order -> sorted position (2x2 start blocks per sub-bin)
+  std::vector<float2> vph;         // sorted order: exp(i (om_y + om_x) / 2)
   std::vector<int32_t> sb_off;     // nkeys+1
   std::vector<int64_t> block_sizes;
   int64_t M = 0;
@@ -85,6 +100,8 @@ struct MeasOp {
   DevBuf<float4> geom;
   DevBuf<float2> zbuf;      // pass-1 output z of the l2-ball dual update
   DevBuf<int32_t> perm;
+  DevBuf<int32_t> gperm;    // [Mtot] channel-relative sorted position of the k-th visibility in gridding order
+  DevBuf<float2> vph;       // [Mtot] per-visibility tap phase (sorted order)
   DevBuf<int32_t> sb_off;
   DevBuf<int64_t> ch_voff;
   DevBuf<int32_t> ch_M, ch_blkoff, ch_nblk;
@@ -112,6 +129,8 @@ struct MeasOp {
   std::vector<int> h_dg_off, h_gr_off;   // [L+1] item offsets per channel
   DevBuf<int> dg_off;                    // device copy of h_dg_off
   DevBuf<GridCombine> gr_combine;
+  DevBuf<int> gr_order;                  // gridding items, largest first (whole-operator launches)
+  DevBuf<GridPlan> gr_plan;              // [gridding items] sub-bin schedules
   std::vector<int> h_comb_off;           // [L+1] combine entries per channel
   DevBuf<float2> gr_partial;             // [partial slots][tile cells]
   DevBuf<double> blk_stats; // [nblk_tot][2]: ||z||^2, ||res||^2

@@ -165,6 +165,7 @@ MinMaxAxis build_minmax_axis(int N, int K, int J, int n_samples, int n_cos) {
   // table h[j][t], dk = J/2 + t/n_samples
   ax.table_re.assign((size_t)J * (n_samples + 1), 0.0);
   ax.table_im.assign((size_t)J * (n_samples + 1), 0.0);
+  std::vector<double> table_c((size_t)J * (n_samples + 1), 0.0);  // c_j(dk), real
   std::vector<double> r(J), cc(J);
   for (int ti = 0; ti <= n_samples; ++ti) {
     const double dk = J / 2.0 + (double)ti / n_samples;
@@ -179,6 +180,7 @@ MinMaxAxis build_minmax_axis(int N, int K, int J, int n_samples, int n_cos) {
       cc[j] = acc;
     }
     for (int j = 1; j <= J; ++j) {
+      table_c[(size_t)(j - 1) * (n_samples + 1) + ti] = cc[j - 1];
       const double ph = M_PI / K * (dk - j);
       ax.table_re[(size_t)(j - 1) * (n_samples + 1) + ti] = std::cos(ph) * cc[j - 1];
       ax.table_im[(size_t)(j - 1) * (n_samples + 1) + ti] = std::sin(ph) * cc[j - 1];
@@ -203,6 +205,12 @@ MinMaxAxis build_minmax_axis(int N, int K, int J, int n_samples, int n_cos) {
       const std::vector<double> c = lstsq(V, t, m, nt);
       for (int k = 0; k < nt; ++k) ax.poly[((size_t)j * 2 + part) * nt + k] = c[k];
     }
+  ax.poly_real.assign((size_t)J * nt, 0.0);
+  for (int j = 0; j < J; ++j) {
+    std::vector<double> t(table_c.begin() + (size_t)j * m, table_c.begin() + (size_t)(j + 1) * m);
+    const std::vector<double> c = lstsq(V, t, m, nt);
+    for (int k = 0; k < nt; ++k) ax.poly_real[(size_t)j * nt + k] = c[k];
+  }
   return ax;
 }
 

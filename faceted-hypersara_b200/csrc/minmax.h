@@ -14,6 +14,9 @@ struct MinMaxAxis {
   // degree kPolyDegree least-squares polynomials of every tap in
   // s = (dk - J/2) - 1/2 in [-1/2, 1/2): poly[(j*2 + part)*(kPolyDegree+1) + k]
   std::vector<double> poly;
+  // the same taps without their phase: h_j(dk) = exp(i pi (dk - j)/K) c_j(dk)
+  // with c_j real; degree kPolyDegree fits poly_real[j*(kPolyDegree+1) + k]
+  std::vector<double> poly_real;
 };
 
 constexpr int kPolyDegree = 8;
