@@ -62,6 +62,7 @@ class RunInfo(C.Structure):
 
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
 _i64p = C.POINTER(C.c_int64)
 
@@ -115,6 +116,14 @@ SIGNATURES = {
     "fhs_solver_iterate": (C.c_int, [_vp, C.c_int, C.POINTER(IterInfo)]),
     "fhs_solver_run": (C.c_int, [_vp, C.c_int, C.POINTER(RunInfo)]),
     "fhs_solver_get_x": (C.c_int, [_vp, _dp]),
+    "fhs_unet_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(_vp)]),
+    "fhs_unet_destroy": (C.c_int, [_vp]),
+    "fhs_unet_n_params": (C.c_int64, [_vp]),
+    "fhs_unet_set_params": (C.c_int, [_vp, _fp]),
+    "fhs_unet_get_params": (C.c_int, [_vp, _fp]),
+    "fhs_unet_forward": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp]),
+    "fhs_unet_gradient": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _dp]),
+    "fhs_unet_train_step": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp, C.c_float, _dp]),
     "fhs_solver_group_stats": (C.c_int, [_vp, _dp]),
     "fhs_solver_update_weights": (C.c_int, [_vp]),
     "fhs_solver_ellipse_iterations": (C.c_int, [_vp, C.POINTER(C.c_int)]),

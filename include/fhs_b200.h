@@ -377,6 +377,34 @@ FHS_API fhs_status fhs_solver_group_stats(fhs_solver* s, double* out);
 /* Recompute reweighting weights from the current x (fhs_update_weights.m). */
 FHS_API fhs_status fhs_solver_update_weights(fhs_solver* s);
 
+/* ======================================================================
+ * Learned warm start (no counterpart in the reference; its output is the
+ * xinit / varargin{1} of facetHyperSARA.m:1-6, hyperSARA.m:1-3 and
+ * sara.m:1-3, used at facetHyperSARA.m:347-350).  A BF16 U-Net (4 levels,
+ * 32 base channels, 2,140,065 parameters) maps one normalised dirty image
+ * to an initial estimate; trained and run by the library's own kernels.
+ * Images are float [n][H][W] (W fastest), H and W multiples of 8; each
+ * image is scaled by 1 / max|image| on the way in and its output by the
+ * inverse on the way out.  Parameters: a flat float vector, per 3x3 layer
+ * (in forward order) weight [Cout][Cin][3][3] then bias [Cout], then the
+ * 1x1 head weight [32] and bias [1].
+ * ====================================================================== */
+typedef struct fhs_unet fhs_unet;
+FHS_API fhs_status fhs_unet_create(int device, int base_channels, fhs_unet** out);
+FHS_API fhs_status fhs_unet_destroy(fhs_unet* net);
+FHS_API int64_t fhs_unet_n_params(const fhs_unet* net);
+FHS_API fhs_status fhs_unet_set_params(fhs_unet* net, const float* params);
+FHS_API fhs_status fhs_unet_get_params(fhs_unet* net, float* params);
+/* out[n][H][W] = network(images) */
+FHS_API fhs_status fhs_unet_forward(fhs_unet* net, int n_images, int H, int W, const float* images, float* out);
+/* loss = mean((s (out - target))^2) over all pixels (s the image's input
+ * scale) and its gradient with respect to every parameter (grad may be NULL) */
+FHS_API fhs_status fhs_unet_gradient(fhs_unet* net, int n_images, int H, int W, const float* images,
+                                     const float* targets, float* grad, double* loss);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss above */
+FHS_API fhs_status fhs_unet_train_step(fhs_unet* net, int n_images, int H, int W, const float* images,
+                                       const float* targets, float lr, double* loss);
+
 /* Measurement hooks (no reference counterpart: the reference times its
  * phases with tic/toc, src/fhs/facetHyperSARA.m:703-716,771-776).
  * time_iterations: n graph replays bracketed by CUDA events on the solver's

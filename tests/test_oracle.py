@@ -327,3 +327,12 @@ def test_noise_adjustment_rule_and_trigger():
     assert loga.n_adjust >= 1 and loga.epsilon[1] > 10 * loga.epsilon[0]
     assert all(e1 >= e0 for el0, el1 in zip(data.eps, loga.epsilon_final) for e0, e1 in zip(el0, el1))
     assert logb.epsilon[-1] == logb.epsilon[0] and not np.allclose(xa, xb)
+
+
+def test_warm_start_network_layout_matches_the_oracle():
+    """The product's U-Net layer list and parameter count equal the oracle's
+    (the gradient check relies on one flat parameter layout)."""
+    from fhs_b200 import warmstart
+    from oracle import unet
+    assert warmstart.layer_specs() == unet.layer_specs()
+    assert warmstart.init_params().size == unet.n_params() == 2140065
