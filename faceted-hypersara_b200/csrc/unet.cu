@@ -11,7 +11,10 @@
 // 2x2 average pooling between them; decoder levels that upsample (nearest,
 // 2x), convolve (3x3 + ReLU) to the level's width, concatenate the encoder
 // feature map of that level and apply two more 3x3 convolutions + ReLU; a
-// 1x1 convolution to one channel plus the input image (residual output).
+// 1x1 convolution to one channel.  No residual path to the input: the
+// normalised dirty image is about the beam area (tens of pixels) times
+// larger than the sky it maps to, so an identity path only has to be
+// cancelled first.
 //
 // Kernels:
 //  * conv3x3_kernel: implicit GEMM on the tensor cores (mma.sync m16n8k16,
@@ -309,7 +312,7 @@ __global__ void image_to_nhwc_kernel(const float* __restrict__ img, const float*
     out[i] = __float2bfloat16(img[i] * scale[i / npix]);
 }
 
-// out[n][y][x] = sum_c f[p][c] wh[c] + bh + in_scaled[p], then / scale[n]
+// out[n][y][x] = (sum_c f[p][c] wh[c] + bh) / scale[n]
 __global__ void head_fwd_kernel(const bf16* __restrict__ f, int C, const float* __restrict__ wh, const float* bh,
                                 const float* __restrict__ img, const float* __restrict__ scale, int npix, int nimg,
                                 float* __restrict__ out) {
@@ -317,8 +320,7 @@ __global__ void head_fwd_kernel(const bf16* __restrict__ f, int C, const float* 
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float s = bh[0];
     for (int c = 0; c < C; ++c) s = fmaf(__bfloat162float(f[i * C + c]), wh[c], s);
-    const float sc = scale[i / npix];
-    out[i] = (s + img[i] * sc) / sc;
+    out[i] = s / scale[i / npix];
   }
 }
 

@@ -44,8 +44,7 @@ def layer_specs(b=N_BASE):
 
 
 def init_params(seed=0, b=N_BASE):
-    """He-normal 3x3 weights, zero biases, a small head (the network starts
-    close to its residual path: the scaled input)."""
+    """He-normal 3x3 weights, zero biases, a small head (outputs start near 0)."""
     rng = np.random.default_rng(seed)
     out = []
     for ci, co in layer_specs(b):

@@ -11,8 +11,8 @@ Architecture (4 levels, 32 base channels): encoder levels of two 3x3
 convolutions + ReLU (32, 64, 128, 256 channels) with 2x2 average pooling in
 between; decoder levels of a nearest 2x upsample, a 3x3 convolution + ReLU,
 concatenation with the encoder map of the level, and two 3x3 convolutions +
-ReLU; a 1x1 convolution to one channel plus the scaled input.  Inputs are
-scaled by s = 1 / max|image| per image; the output is divided by s again.
+ReLU; a 1x1 convolution to one channel.  Inputs are scaled by
+s = 1 / max|image| per image; the output is divided by s again.
 The loss is mean((s (out - target))^2) over all pixels.
 """
 from __future__ import annotations
@@ -31,8 +31,7 @@ def n_params(b=32):
 
 
 def init_params(seed=0, b=32):
-    """He-normal weights, zero biases, head weight small (starts near the
-    identity map of the residual output)."""
+    """He-normal weights, zero biases, head weight small (outputs start near 0)."""
     rng = np.random.default_rng(seed)
     out = []
     for ci, co in layer_specs(b):
@@ -87,7 +86,6 @@ def forward(params, images, b=32, bf16=False, dtype=None):
     def up(t):
         return F.interpolate(t, scale_factor=2, mode="nearest")
 
-    x_in = x
     x = r(x)
     e1 = conv(conv(x, 0), 1)
     e2 = conv(conv(pool(e1), 2), 3)
@@ -100,7 +98,7 @@ def forward(params, images, b=32, bf16=False, dtype=None):
     u1 = conv(up(d2), 14)
     d1 = conv(conv(torch.cat([u1, e1], 1), 15), 16)
     head = F.conv2d(d1, hw, hb)[:, 0]
-    out = (head + x_in[:, 0]) / s[:, None, None]   # the residual uses the unrounded scaled input
+    out = head / s[:, None, None]
     return out, s
 
 
