@@ -1034,9 +1034,16 @@ __global__ void pad_real_kernel(const float* __restrict__ x, float* __restrict__
 }
 
 void measop_enable_r2c(MeasOp* op) {
-  if (op->plan_r2c) return;
+  if (op->plan_r2c || op->own_fft) return;
   DeviceGuard g(op->device);
   cudaStream_t s = op->stream;
+  if (measop_own_fft(op)) {   // the hand-written transforms of fft.cu
+    measop_fft_tables(op, s);
+    op->imgr.alloc((size_t)op->L * op->Npix());
+    op->own_fft = true;
+    FHS_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
   op->padr.alloc((size_t)op->L * op->No());
   op->padr.zero(s);
   op->imgr.alloc((size_t)op->L * op->No());
@@ -1073,6 +1080,21 @@ void fft_inverse_c2r(const MeasOp* op, cudaStream_t s) {
   count_launch();
   FHS_LAUNCH_CHECK();
   FHS_CUFFT(cufftExecC2R(op->plan_c2r, (cufftComplex*)op->gridA.p, op->imgr.p));
+}
+
+void solver_fft_forward(const MeasOp* op, const float* x, cudaStream_t s) {
+  if (op->own_fft) {
+    fft_forward_half(op, x, 0, op->L, s);
+  } else {
+    fft_forward_r2c(op, s);   // reads the padded image written by the caller
+  }
+}
+
+void solver_fft_inverse(const MeasOp* op, cudaStream_t s) {
+  if (op->own_fft)
+    fft_inverse_real(op, op->imgr.p, 0, op->L, s);
+  else
+    fft_inverse_c2r(op, s);
 }
 
 void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s) {

@@ -118,6 +118,10 @@ struct MeasOp {
   // real inverse FFT [L][Kx][Ky]
   DevBuf<float> imgr;
   cufftHandle plan_c2r = 0;
+  // hand-written FFTs of the solvers' real-image path (fft.cu), for
+  // power-of-two grid sides 64..4096: twiddle tables exp(-2 pi i k / K)
+  bool own_fft = false;
+  DevBuf<float2> tw_y, tw_x;
 
   // scratch for API-level calls
   DevBuf<float2> vis_a, vis_b;
@@ -194,6 +198,17 @@ void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStrea
 void fft_forward_r2c(const MeasOp* op, cudaStream_t s);
 // imgr <- Re(IFFT(gridB)) of all L planes (Hermitian half into gridA, then C2R)
 void fft_inverse_c2r(const MeasOp* op, cudaStream_t s);
+// hand-written transforms (fft.cu): power-of-two grid sides 64..4096
+bool measop_own_fft(const MeasOp* op);
+void measop_fft_tables(MeasOp* op, cudaStream_t s);
+// x: planes p0.. of the image [L][Nx][Ny] -> gridA half spectrum [L][Kx][Ky/2+1]
+void fft_forward_half(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s);
+// gridB [L][Kx][Ky] -> out: planes p0.. of Re(At gridB) on the image, [L][Nx][Ny], unscaled
+void fft_inverse_real(const MeasOp* op, float* out, int p0, int np, cudaStream_t s);
+// the solvers' real-image transforms: the hand-written ones when op->own_fft
+// (imgr then holds [L][Nx][Ny]), else padr -> cuFFT R2C and C2R -> imgr [L][Kx][Ky]
+void solver_fft_forward(const MeasOp* op, const float* x, cudaStream_t s);
+void solver_fft_inverse(const MeasOp* op, cudaStream_t s);
 // gridB <- G^H v (v sorted, channels [c0, c0+nc)); non-empty tiles only
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
 // out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1

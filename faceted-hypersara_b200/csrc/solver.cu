@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, 
   float* xp = x + (size_t)plane * N;
   const float* gp = g + (size_t)plane * N;
   float* hp = xhat + (size_t)plane * N;
-  float* pp = pad + (size_t)plane * Ky * Kx;
+  float* pp = pad ? pad + (size_t)plane * Ky * Kx : nullptr;
   double a = 0.0, b = 0.0;
   // four pixels per step (N is a multiple of 4: Ny and Nx are even), float4
   // loads and stores of x, g and xhat for memory-level parallelism
@@ -76,13 +76,15 @@ __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, 
       const double d = (double)xo[e] - xn[e];
       a += d * d;
       b += (double)xn[e] * xn[e];
-      const int64_t p = 4 * q + e;
-      const int ix = (int)(p / Ny), iy = (int)(p - (int64_t)ix * Ny);
-      int ky = iy - Ny / 2;
-      ky += ky < 0 ? Ky : 0;
-      int kx = ix - Nx / 2;
-      kx += kx < 0 ? Kx : 0;
-      pp[(size_t)kx * Ky + ky] = xn[e] * sy[iy] * sx[ix];
+      if (pad) {   // the padded image of the cuFFT path (the hand-written FFT reads x)
+        const int64_t p = 4 * q + e;
+        const int ix = (int)(p / Ny), iy = (int)(p - (int64_t)ix * Ny);
+        int ky = iy - Ny / 2;
+        ky += ky < 0 ? Ky : 0;
+        int kx = ix - Nx / 2;
+        kx += kx < 0 ? Kx : 0;
+        pp[(size_t)kx * Ky + ky] = xn[e] * sy[iy] * sx[ix];
+      }
     }
     reinterpret_cast<float4*>(xp)[q] = make_float4(xn[0], xn[1], xn[2], xn[3]);
     reinterpret_cast<float4*>(hp)[q] = make_float4(xh[0], xh[1], xh[2], xh[3]);
@@ -96,6 +98,7 @@ __global__ void __launch_bounds__(256) primal_pad_kernel(float* __restrict__ x, 
 
 struct AssembleArgs {
   int Ny, Nx, Ky, Kx, lg, Qy, nuclear;
+  int img_compact;   // img holds [L][Nx][Ny] (hand-written FFT) instead of [L][Kx][Ky]
   float sigma00;
   const NucFacet* facets;
   const float* wy;
@@ -122,7 +125,8 @@ __global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, int L, fl
     ky += ky < 0 ? a.Ky : 0;
     int kx = ix - a.Nx / 2;
     kx += kx < 0 ? a.Kx : 0;
-    const int64_t kimg = (int64_t)kx * a.Ky + ky;
+    const int64_t kimg = a.img_compact ? p : (int64_t)kx * a.Ky + ky;
+    const int64_t pstride = a.img_compact ? N : plane_img;
     const float syi = sy[iy], sxi = sx[ix];
     int ne = 0;
     int64_t base[4], P[4];
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(AssembleArgs a, int L, fl
     }
     for (int plane = 0; plane < L; ++plane) {
       const int grp = plane / a.lg, lc = plane - grp * a.lg;
-      float val = sigma22[plane] * syi * sxi * img[(size_t)plane * plane_img + kimg] + g1[(size_t)plane * N + p];
+      float val = sigma22[plane] * syi * sxi * img[(size_t)plane * pstride + kimg] + g1[(size_t)plane * N + p];
       if (ne) {
         float acc = 0.f;
         const float* vg = v0 + (int64_t)grp * a.v0_group;
@@ -277,12 +281,13 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
     ++stage;
   };
   mark();
-  primal_pad_kernel<<<dim3(kPrimalBlocks, L), 256, 0, s>>>(S->x.p, S->g.p, S->xhat.p, op->padr.p, op->sy.p,
+  primal_pad_kernel<<<dim3(kPrimalBlocks, L), 256, 0, s>>>(S->x.p, S->g.p, S->xhat.p,
+                                                           op->own_fft ? nullptr : op->padr.p, op->sy.p,
                                                            op->sx.p, S->Ny, S->Nx, op->Ky, op->Kx, S->primal_part.p);
   count_launch();
   FHS_LAUNCH_CHECK();
   mark();
-  fft_forward_r2c(op, s);
+  solver_fft_forward(op, S->x.p, s);
   mark();
   if (S->precond) {
     launch_degrid_dual_precond(op, 0, L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s, true);
@@ -302,7 +307,7 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
     launch_grid_dual(op, 0, L, S->v2.p, s);
     mark();
   }
-  fft_inverse_c2r(op, s);
+  solver_fft_inverse(op, s);
   mark();
   FHS_CUDA(cudaMemsetAsync(S->l21_acc.p, 0, S->G * sizeof(double), s));
   if (sara_fused_supported(S->lg)) {
@@ -330,6 +335,7 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
   a.lg = S->lg;
   a.Qy = S->nuclear ? S->np.Qy : 1;
   a.nuclear = S->nuclear ? 1 : 0;
+  a.img_compact = op->own_fft ? 1 : 0;
   a.sigma00 = (float)S->sigma00;
   a.facets = S->nuclear ? S->np.d_facets.p : nullptr;
   a.wy = S->nuclear ? S->np.wy.p : nullptr;
@@ -643,8 +649,8 @@ fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
     if (S->nuclear) S->v0.zero(s);
     S->ring_counter.zero(s);
     // Fx_old: keep G A x_init per visibility (linearity of G)
-    launch_pad_real(op, S->x.p, 0, S->L, s);
-    fft_forward_r2c(op, s);
+    if (!op->own_fft) launch_pad_real(op, S->x.p, 0, S->L, s);
+    solver_fft_forward(op, S->x.p, s);
     launch_degrid_plain(op, 0, S->L, S->gold.p, s, true);
     S->precond = op->precond;
     if (S->precond) {
