@@ -122,22 +122,25 @@ __device__ __forceinline__ uint4 load_in8(const ConvArgs& a, int n, int y, int x
 
 // 3x3 convolution, stride 1, zero padding 1 (cross-correlation, as the
 // usual deep-learning convention), implicit GEMM: M = pixels, N = Cout,
-// K = 9 * Cpad.  128 threads: warp w owns pixels 32 (w & 1) + [0, 32) and
-// channels 32 (w >> 1) + [0, 32) of the CTA tile.
+// K = 9 * Cpad.  CT output channels per CTA (64, or 32 for the 32-channel
+// layers); 128 threads: warp w owns pixels 32 (w & 1) + [0, 32) and channels
+// (CT / 2) (w >> 1) + [0, CT / 2) of the CTA tile.
+template <int CT>
 __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs a) {
+  constexpr int NB = CT / 16;   // n8 blocks per warp
   extern __shared__ __align__(16) unsigned char conv_sm[];
   bf16* halo = reinterpret_cast<bf16*>(conv_sm);                 // [100][kPitch]
-  bf16* wsm = halo + kHalo * kHalo * kPitch;                      // [kCT][9][kPitch]
+  bf16* wsm = halo + kHalo * kHalo * kPitch;                      // [CT][9][kPitch]
   const int tiles_x = (a.W + 7) >> 3;
   const int ty0 = (blockIdx.x / tiles_x) * 8, tx0 = (blockIdx.x % tiles_x) * 8;
-  const int n = blockIdx.y, co0 = blockIdx.z * kCT;
+  const int n = blockIdx.y, co0 = blockIdx.z * CT;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ph = warp & 1, chf = warp >> 1;
-  float acc[2][4][4];
+  float acc[2][NB][4];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < NB; ++j)
 #pragma unroll
       for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.f;
   for (int cc = 0; cc < a.Cpad; cc += kCK) {
@@ -146,7 +149,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs a) {
       const int hy = hp / kHalo, hx = hp - hy * kHalo;
       *reinterpret_cast<uint4*>(halo + hp * kPitch + g * 8) = load_in8(a, n, ty0 + hy - 1, tx0 + hx - 1, cc + g * 8);
     }
-    for (int t = threadIdx.x; t < kCT * 9 * 4; t += blockDim.x) {
+    for (int t = threadIdx.x; t < CT * 9 * 4; t += blockDim.x) {
       const int g = t & 3, row = t >> 2;   // row = co_local * 9 + tap
       const int col = row / 9, tap = row - col * 9;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
@@ -167,17 +170,17 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs a) {
           const int r = p >> 3, c = p & 7;
           ldsm_x4(af[mb], halo + ((r + dy) * kHalo + (c + dx)) * kPitch + ks * 16 + (lane >> 4) * 8);
         }
-        unsigned bfr[2][4];
+        unsigned bfr[NB / 2][4];
 #pragma unroll
-        for (int np = 0; np < 2; ++np) {
+        for (int np = 0; np < NB / 2; ++np) {
           const int mi = lane >> 3;
-          const int co = chf * 32 + np * 16 + ((mi >> 1) << 3) + (lane & 7);
+          const int co = chf * (CT / 2) + np * 16 + ((mi >> 1) << 3) + (lane & 7);
           ldsm_x4(bfr[np], wsm + (co * 9 + tap) * kPitch + ks * 16 + (mi & 1) * 8);
         }
 #pragma unroll
         for (int mb = 0; mb < 2; ++mb)
 #pragma unroll
-          for (int nb = 0; nb < 4; ++nb)
+          for (int nb = 0; nb < NB; ++nb)
             mma_bf16(acc[mb][nb], af[mb], bfr[nb >> 1][(nb & 1) * 2], bfr[nb >> 1][(nb & 1) * 2 + 1]);
       }
     }
@@ -193,8 +196,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs a) {
       if (y >= a.H || x >= a.W) continue;
       bf16* op = a.out + (((size_t)n * a.H + y) * a.W + x) * a.out_pitch;
 #pragma unroll
-      for (int nb = 0; nb < 4; ++nb) {
-        const int co = co0 + chf * 32 + nb * 8 + 2 * tq;
+      for (int nb = 0; nb < NB; ++nb) {
+        const int co = co0 + chf * (CT / 2) + nb * 8 + 2 * tq;
         float v0 = acc[mb][nb][half * 2], v1 = acc[mb][nb][half * 2 + 1];
         if (a.bias) {
           if (co < a.Cout) v0 += a.bias[co];
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs a) {
     }
 }
 
-constexpr size_t kConvSmem = (size_t)(kHalo * kHalo + kCT * 9) * kPitch * sizeof(bf16);
+constexpr size_t kConvSmem = (size_t)(kHalo * kHalo + kCT * 9) * kPitch * sizeof(bf16);   // CT = 64
 
 // Weight gradient of a 3x3 convolution: dW[co][tap][ci] += sum over pixels
 // of g[p][co] in[p + offset(tap)][ci].  CTA: 64 output channels x 32 input
@@ -589,9 +592,13 @@ void conv(UNet* u, const UNetLayer& L, TView in0, TView in1, int up, int N, int 
   a.out = out;
   a.out_pitch = out_pitch;
   (void)L;
-  dim3 grid(((W + 7) / 8) * ((H + 7) / 8), N, (cout + kCT - 1) / kCT);
+  const int ct = cout <= 32 ? 32 : kCT;   // the 32-channel layers use half-width tiles
+  dim3 grid(((W + 7) / 8) * ((H + 7) / 8), N, (cout + ct - 1) / ct);
   FHS_CHECK(grid.y <= 65535 && grid.z <= 65535, FHS_ERR_UNSUPPORTED, "batch too large");
-  conv3x3_kernel<<<grid, 128, kConvSmem, u->stream>>>(a);
+  if (ct == 32)
+    conv3x3_kernel<32><<<grid, 128, (size_t)(kHalo * kHalo + 32 * 9) * kPitch * sizeof(bf16), u->stream>>>(a);
+  else
+    conv3x3_kernel<64><<<grid, 128, kConvSmem, u->stream>>>(a);
   count_launch();
   FHS_LAUNCH_CHECK();
 }
@@ -641,12 +648,7 @@ void ensure_batch(UNet* u, int N, int H, int W) {
     u->act.emplace_back(new DevBuf<bf16>());
     u->act.back()->alloc(sz[i]);
   }
-  // gradient scratch: two ping-pong buffers of the largest map (2b channels at full size covers every concat)
-  u->gbuf.clear();
-  for (int i = 0; i < 4; ++i) {
-    u->gbuf.emplace_back(new DevBuf<bf16>());
-    u->gbuf.back()->alloc(p0 * 2 * b);
-  }
+  u->gbuf.clear();   // gradient scratch, allocated by the first backward pass of this batch size
   u->img.alloc(p0);
   u->tgt.alloc(p0);
   u->outp.alloc(p0);
@@ -708,6 +710,12 @@ void backward(UNet* u) {
   const int N = u->N, H = u->H, W = u->W, b = u->base;
   cudaStream_t s = u->stream;
   const int64_t p0 = (int64_t)N * H * W;
+  if (u->gbuf.empty()) {   // four maps of 2b channels at full size cover every gradient and concat
+    for (int i = 0; i < 4; ++i) {
+      u->gbuf.emplace_back(new DevBuf<bf16>());
+      u->gbuf.back()->alloc(p0 * 2 * b);
+    }
+  }
   u->grad.zero(s);
   for (auto& L : u->conv) L->dwp.zero(s);
   u->loss.zero(s);
@@ -832,7 +840,7 @@ fhs_status fhs_unet_create(int device, int base_channels, fhs_unet** out) {
     u->device = device;
     u->base = base_channels;
     FHS_CUDA(cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking));
-    FHS_CUDA(cudaFuncSetAttribute(conv3x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmem));
+    FHS_CUDA(cudaFuncSetAttribute(conv3x3_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmem));
     int64_t off = 0;
     for (const auto& sp : layer_specs(base_channels)) {
       std::unique_ptr<UNetLayer> L(new UNetLayer());

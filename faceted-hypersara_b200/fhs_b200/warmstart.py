@@ -149,7 +149,7 @@ def dirty_cube(op, y):
     return compute_residual_images(np.zeros((op.Ny, op.Nx, op.L)), y, op)
 
 
-def network_cube(net: UNet, cube, chunk=4):
+def network_cube(net: UNet, cube, chunk=16):
     """Apply the network to every channel of a cube [Ny, Nx, L] (images are
     [Nx, Ny] in the network's row-major convention), clipped at 0 as the
     primal update of the solvers does (fhs_update_primal.m:33-38)."""
