@@ -454,7 +454,8 @@ def run_ours(args):
                 if args.precond else ("visibility gridding (DR), l2 ball, 1 block per channel; stages "
                                       "degrid_dual / grid_dual are the two DR stencil passes" if args.dr
                                       else "l2 ball (pU = 1)"),
-                "vis_per_s": 2.0 * prob["n_vis"] * value}
+                "vis_per_s": 2.0 * prob["n_vis"] * value,
+                "tuning": prob["op"].tuning()}
         print(json.dumps(line), flush=True)
     s.close()
     prob["op"].close()

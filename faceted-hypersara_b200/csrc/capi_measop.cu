@@ -70,9 +70,14 @@ static void forward_impl(MeasOp* op, const double* x, double* y, bool precond) {
   float2* va = vis_scratch(op, op->vis_a);
   FHS_CUDA(cudaMemcpyAsync(st, x, N * op->L * sizeof(double), cudaMemcpyHostToDevice, s));
   launch_d2f(st, img, N * op->L, s);
-  launch_pad(op, img, 0, op->L, s);
-  fft_forward(op, 0, op->L, s);
-  launch_degrid_plain(op, 0, op->L, va, s);
+  if (op->tw_y.p) {   // hand-written real-to-half-spectrum transforms
+    fft_forward_half(op, img, 0, op->L, s);
+    launch_degrid_plain(op, 0, op->L, va, s, true);
+  } else {
+    launch_pad(op, img, 0, op->L, s);
+    fft_forward(op, 0, op->L, s);
+    launch_degrid_plain(op, 0, op->L, va, s);
+  }
   if (precond) launch_scale_pu(op, va, true, s);
   launch_vis_scatter(va, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
   FHS_CUDA(cudaMemcpyAsync(y, st, 2 * op->Mtot * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -94,8 +99,13 @@ static void adjoint_impl(MeasOp* op, const double* y, double* x, bool precond) {
   launch_vis_gather(st, va, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
   if (precond) launch_scale_pu(op, va, true, s);
   launch_grid_plain(op, 0, op->L, va, s);
-  fft_inverse(op, 0, op->L, s);
-  launch_crop_real(op, img, nullptr, 0, op->L, s);
+  if (op->tw_y.p) {   // hand-written spectrum-to-real transforms
+    fft_inverse_real(op, img, 0, op->L, s);
+    launch_scale_image(op, img, op->L, s);
+  } else {
+    fft_inverse(op, 0, op->L, s);
+    launch_crop_real(op, img, nullptr, 0, op->L, s);
+  }
   launch_f2d(img, st, N * op->L, s);
   FHS_CUDA(cudaMemcpyAsync(x, st, N * op->L * sizeof(double), cudaMemcpyDeviceToHost, s));
   FHS_CUDA(cudaStreamSynchronize(s));
@@ -246,6 +256,51 @@ fhs_status fhs_measop_dr_cells(fhs_measop* op_, int channel, int64_t* cells) {
     op->dr_cell.download_at(h.data(), op->h_voff[channel], n, op->stream);
     FHS_CUDA(cudaStreamSynchronize(op->stream));
     for (int64_t i = 0; i < n; ++i) cells[i] = h[i];
+  });
+}
+
+static void tuning_record(const MeasOp* op, fhs_tuning* t) {
+  *t = fhs_tuning{};
+  t->tuned = op->tuned ? 1 : 0;
+  t->fft_chunk = op->own_fft || op->tw_y.p ? op->fft_chunk : -1;
+  t->grid_slice = op->dr ? 0 : op->grid_slice;
+  t->n_fft = (int)std::min<size_t>(op->tune_fft.size(), FHS_TUNING_MAX_CANDIDATES);
+  for (int i = 0; i < t->n_fft; ++i) {
+    t->fft_candidates[i] = op->tune_fft[i].first;
+    t->fft_ms[i] = op->tune_fft[i].second;
+  }
+  t->n_grid = (int)std::min<size_t>(op->tune_grid.size(), FHS_TUNING_MAX_CANDIDATES);
+  for (int i = 0; i < t->n_grid; ++i) {
+    t->grid_candidates[i] = op->tune_grid[i].first;
+    t->grid_ms[i] = op->tune_grid[i].second;
+  }
+}
+
+fhs_status fhs_measop_autotune(fhs_measop* op_, fhs_tuning* out) {
+  return guarded([&] {
+    MeasOp* op = committed(op_);
+    measop_autotune(op);
+    if (out) tuning_record(op, out);
+  });
+}
+
+fhs_status fhs_measop_set_tuning(fhs_measop* op_, int fft_chunk, int grid_slice) {
+  return guarded([&] {
+    MeasOp* op = committed(op_);
+    FHS_CHECK(fft_chunk >= 0 && grid_slice >= 1024, FHS_ERR_INVALID_ARG, "fft_chunk >= 0, grid_slice >= 1024");
+    measop_set_grid_slice(op, grid_slice);
+    op->fft_chunk = fft_chunk;
+    op->tune_fft.clear();
+    op->tune_grid.clear();
+    op->tuned = true;
+    ++op->layout_epoch;
+  });
+}
+
+fhs_status fhs_measop_tuning(const fhs_measop* op_, fhs_tuning* out) {
+  return guarded([&] {
+    FHS_CHECK(out != nullptr, FHS_ERR_INVALID_ARG, "null output");
+    tuning_record(committed(const_cast<fhs_measop*>(op_)), out);
   });
 }
 

@@ -811,12 +811,11 @@ void measop_set_channel(MeasOp* op, int c, int64_t n, const double* om_y, const 
 // Work lists for the tile kernels.  Degridding: one item per non-empty
 // (channel, tile), split into slices of at most kDegridSlice visibilities.
 // Gridding: one item per (channel, tile) whose footprint ring holds any
-// visibility, split into slices of at most kGridSlice; split tiles get partial
+// visibility, split into slices of at most op->grid_slice; split tiles get partial
 // tiles that grid_combine_kernel sums.  Empty tiles are never written (the
 // gridding output is zeroed at commit).  Items run channel by channel in tile
 // order, so neighbouring tiles (which share aprons) run close together.
 constexpr int kDegridSlice = 8192;
-constexpr int kGridSlice = 32768;
 
 static void build_work_lists(MeasOp* op, cudaStream_t s) {
   const int L = op->L, nt = op->ntiles();
@@ -872,7 +871,7 @@ static void build_work_lists(MeasOp* op, cudaStream_t s) {
           for (const auto& e : ph[q]) plan.sub[pos++] = (uint8_t)e.second;
         }
       }
-      const int ns = (tot + kGridSlice - 1) / kGridSlice;
+      const int ns = (tot + op->grid_slice - 1) / op->grid_slice;
       if (ns == 1) {
         gr.push_back(WorkItem{c, t, 0, 1, -1, 0});
         gr_work.push_back(tot);
@@ -912,6 +911,16 @@ static void build_work_lists(MeasOp* op, cudaStream_t s) {
   op->gr_partial.alloc(std::max<size_t>((size_t)pslot * kTileCells * kTileCells, 1));
   op->partials.alloc(std::max<size_t>(dg.size(), 1) * kMaxBlocksPerChannel * 2);
   FHS_CUDA(cudaStreamSynchronize(s));
+}
+
+void measop_set_grid_slice(MeasOp* op, int slice) {
+  FHS_CHECK(slice >= 1024, FHS_ERR_INVALID_ARG, "gridding slice below 1024 visibilities");
+  if (op->dr || slice == op->grid_slice) return;
+  DeviceGuard g(op->device);
+  FHS_CUDA(cudaStreamSynchronize(op->stream));
+  op->grid_slice = slice;
+  build_work_lists(op, op->stream);
+  ++op->layout_epoch;
 }
 
 void measop_commit(MeasOp* op) {
@@ -1008,6 +1017,7 @@ void measop_commit(MeasOp* op) {
   FHS_CUFFT(cufftSetStream(op->plan_all, s));
   FHS_CUFFT(cufftPlanMany(&op->plan_one, 2, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 1));
   FHS_CUFFT(cufftSetStream(op->plan_one, s));
+  if (measop_own_fft(op)) measop_fft_tables(op, s);   // the hand-written transforms of fft.cu
   FHS_CUDA(cudaStreamSynchronize(s));
   // host copies of the sorted geometry are no longer needed
   for (auto& h : op->ch) {
@@ -1037,8 +1047,7 @@ void measop_enable_r2c(MeasOp* op) {
   if (op->plan_r2c || op->own_fft) return;
   DeviceGuard g(op->device);
   cudaStream_t s = op->stream;
-  if (measop_own_fft(op)) {   // the hand-written transforms of fft.cu
-    measop_fft_tables(op, s);
+  if (op->tw_y.p) {   // the hand-written transforms of fft.cu (tables built at commit)
     op->imgr.alloc((size_t)op->L * op->Npix());
     op->own_fft = true;
     FHS_CUDA(cudaStreamSynchronize(s));
@@ -1084,17 +1093,39 @@ void fft_inverse_c2r(const MeasOp* op, cudaStream_t s) {
 
 void solver_fft_forward(const MeasOp* op, const float* x, cudaStream_t s) {
   if (op->own_fft) {
-    fft_forward_half(op, x, 0, op->L, s);
+    const int step = op->fft_chunk > 0 ? op->fft_chunk : op->L;
+    for (int p0 = 0; p0 < op->L; p0 += step)
+      fft_forward_half(op, x + (size_t)p0 * op->Npix(), p0, std::min(step, op->L - p0), s);
   } else {
     fft_forward_r2c(op, s);   // reads the padded image written by the caller
   }
 }
 
 void solver_fft_inverse(const MeasOp* op, cudaStream_t s) {
-  if (op->own_fft)
-    fft_inverse_real(op, op->imgr.p, 0, op->L, s);
-  else
+  if (op->own_fft) {
+    const int step = op->fft_chunk > 0 ? op->fft_chunk : op->L;
+    for (int p0 = 0; p0 < op->L; p0 += step)
+      fft_inverse_real(op, op->imgr.p + (size_t)p0 * op->Npix(), p0, std::min(step, op->L - p0), s);
+  } else {
     fft_inverse_c2r(op, s);
+  }
+}
+
+__global__ void scale_image_kernel(float* __restrict__ img, const float* __restrict__ sy,
+                                   const float* __restrict__ sx, int Ny, int Nx) {
+  const int64_t N = (int64_t)Ny * Nx;
+  float* p = img + (size_t)blockIdx.y * N;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(i / Ny), iy = (int)(i - (int64_t)ix * Ny);
+    p[i] *= sy[iy] * sx[ix];
+  }
+}
+
+void launch_scale_image(const MeasOp* op, float* img, int np, cudaStream_t s) {
+  dim3 grid(grid_blocks(op->Npix(), 256), np);
+  scale_image_kernel<<<grid, 256, 0, s>>>(img, op->sy.p, op->sx.p, op->Ny, op->Nx);
+  count_launch();
+  FHS_LAUNCH_CHECK();
 }
 
 void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s) {

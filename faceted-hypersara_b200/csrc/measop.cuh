@@ -120,8 +120,19 @@ struct MeasOp {
   cufftHandle plan_c2r = 0;
   // hand-written FFTs of the solvers' real-image path (fft.cu), for
   // power-of-two grid sides 64..4096: twiddle tables exp(-2 pi i k / K)
+  // (tables built at commit when the sizes allow; own_fft: the solvers use them)
   bool own_fft = false;
   DevBuf<float2> tw_y, tw_x;
+  // planes per launch of the solvers' transforms (0: all L at once); smaller
+  // chunks keep each pass's intermediate in L2 for the next pass
+  int fft_chunk = 0;
+  // most visibilities per gridding work item (split items sum partial tiles)
+  int grid_slice = 32768;
+  // bumped whenever work lists or launch shapes change: solvers re-capture
+  int layout_epoch = 0;
+  // autotuner record (fhs_measop_autotune)
+  bool tuned = false;
+  std::vector<std::pair<int, double>> tune_fft, tune_grid;
 
   // scratch for API-level calls
   DevBuf<float2> vis_a, vis_b;
@@ -194,6 +205,10 @@ void launch_degrid_plain(const MeasOp* op, int c0, int nc, float2* out, cudaStre
 // real-to-complex forward path: padr <- s .* x (all planes placed as launch_pad),
 // gridA <- half spectrum of padr (all L planes)
 void measop_enable_r2c(MeasOp* op);
+// rebuild the gridding work lists with at most `slice` visibilities per item
+void measop_set_grid_slice(MeasOp* op, int slice);
+// time the launch-shape candidates and keep the fastest (autotune.cu)
+void measop_autotune(MeasOp* op);
 void launch_pad_real(const MeasOp* op, const float* x, int p0, int np, cudaStream_t s);
 void fft_forward_r2c(const MeasOp* op, cudaStream_t s);
 // imgr <- Re(IFFT(gridB)) of all L planes (Hermitian half into gridA, then C2R)
@@ -213,6 +228,8 @@ void solver_fft_inverse(const MeasOp* op, cudaStream_t s);
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
 // out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1
 void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s);
+// img[p] *= s (the min-max scaling factors sy[iy] sx[ix]), planes [0, np) of a compact [np][Nx][Ny] image
+void launch_scale_image(const MeasOp* op, float* img, int np, cudaStream_t s);
 // fused dual update, pass 1: GFx, z = v2 + 2 GFx - gold - y -> zbuf, GFx -> gold, block partials
 void launch_degrid_dual(const MeasOp* op, int c0, int nc, float2* v2, float2* gold, const float2* y,
                         cudaStream_t s, bool half = false);

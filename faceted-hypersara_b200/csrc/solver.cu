@@ -360,6 +360,7 @@ static void solver_launch_iteration(Solver* S, cudaStream_t s, cudaEvent_t* ev =
 
 static void solver_capture(Solver* S) {
   cudaStream_t s = S->op->stream;
+  S->graph_epoch = S->op->layout_epoch;
   if (S->graph) {
     cudaGraphExecDestroy(S->graph);
     S->graph = nullptr;
@@ -634,6 +635,7 @@ fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
     MeasOp* op = S->op;
     DeviceGuard dg(op->device);
     cudaStream_t s = op->stream;
+    if (!op->tuned) measop_autotune(op);   // before any state: the timed launches use scratch only
     const int64_t n = (int64_t)S->L * S->N;
     if (xinit) {
       if (op->stage.n < (size_t)n) op->stage.alloc(n);
@@ -673,6 +675,12 @@ fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
   });
 }
 
+// the iteration graph holds the operator's work lists and launch shapes:
+// capture it again after the autotuner or fhs_measop_set_tuning changed them
+static void ensure_graph(Solver* S) {
+  if (S->graph_epoch != S->op->layout_epoch) solver_capture(S);
+}
+
 static void read_ring(Solver* S, long long first, int n, std::vector<double>& rec) {
   cudaStream_t s = S->op->stream;
   const size_t per = (size_t)S->G * kReportFields;
@@ -707,6 +715,7 @@ fhs_status fhs_solver_iterate(fhs_solver* s_, int n, fhs_iter_info* info) {
     FHS_CHECK(n >= 0, FHS_ERR_INVALID_ARG, "negative iteration count");
     DeviceGuard dg(S->op->device);
     cudaStream_t s = S->op->stream;
+    ensure_graph(S);
     int done = 0;
     std::vector<double> rec;
     while (done < n) {
@@ -832,6 +841,7 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
     fhs_iter_info info{};
     bool adjust = S->adjust_noise;
     if (adjust) upload_betas(S, true);  // priors off until the first adjustment
+    ensure_graph(S);
     for (t = 1; t <= max_iter; ++t) {
       FHS_CUDA(cudaGraphLaunch(S->graph, s));
       g_launches += S->launches_per_iter;
@@ -1068,6 +1078,7 @@ fhs_status fhs_solver_time_iterations(fhs_solver* s_, int n, double* ms) {
     cudaEvent_t e0, e1;
     FHS_CUDA(cudaEventCreate(&e0));
     FHS_CUDA(cudaEventCreate(&e1));
+    ensure_graph(S);
     FHS_CUDA(cudaStreamSynchronize(s));
     FHS_CUDA(cudaEventRecord(e0, s));
     for (int i = 0; i < n; ++i) FHS_CUDA(cudaGraphLaunch(S->graph, s));

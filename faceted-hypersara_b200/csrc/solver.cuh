@@ -52,6 +52,7 @@ struct Solver {
   bool params_set = false, data_set = false, initialised = false;
 
   cudaGraphExec_t graph = nullptr;
+  int graph_epoch = -1;   // op->layout_epoch the graph was captured at
   unsigned long long launches_per_iter = 0;
   long long iter_done = 0;       // iterations since init
   long long ring_read = 0;       // iterations already read back

@@ -61,6 +61,18 @@ class RunInfo(C.Structure):
                 ("seconds", C.c_double), ("n_noise_adjustments", C.c_int)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("tuned", C.c_int), ("fft_chunk", C.c_int), ("grid_slice", C.c_int), ("n_fft", C.c_int),
+                ("n_grid", C.c_int), ("fft_candidates", C.c_int * 8), ("fft_ms", C.c_double * 8),
+                ("grid_candidates", C.c_int * 8), ("grid_ms", C.c_double * 8)]
+
+    def as_dict(self):
+        return {"tuned": bool(self.tuned), "fft_chunk": self.fft_chunk, "grid_slice": self.grid_slice,
+                "fft_ms": {int(self.fft_candidates[i]): round(float(self.fft_ms[i]), 4) for i in range(self.n_fft)},
+                "grid_ms": {int(self.grid_candidates[i]): round(float(self.grid_ms[i]), 4)
+                            for i in range(self.n_grid)}}
+
+
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
@@ -80,6 +92,9 @@ SIGNATURES = {
     "fhs_measop_is_dr": (C.c_int, [_vp]),
     "fhs_measop_dr_cells": (C.c_int, [_vp, C.c_int, _i64p]),
     "fhs_measop_dr_lambda": (C.c_int, [_vp, C.c_int, _dp]),
+    "fhs_measop_autotune": (C.c_int, [_vp, C.POINTER(Tuning)]),
+    "fhs_measop_set_tuning": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "fhs_measop_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
     "fhs_measop_grid_size": (C.c_int64, [_vp]),
     "fhs_measop_n_blocks": (C.c_int, [_vp, C.c_int]),
     "fhs_measop_image_size": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),

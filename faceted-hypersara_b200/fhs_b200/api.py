@@ -184,6 +184,24 @@ class MeasurementOperator:
         check(fn(self._h, max_iter, tol, dptr(out)))
         return out
 
+    def autotune(self):
+        """Time the launch-shape candidates (FFT planes per launch, gridding
+        work-item size) on this operator and keep the fastest; returns the
+        record of ``tuning()``."""
+        t = LB.Tuning()
+        check(lib().fhs_measop_autotune(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, fft_chunk, grid_slice):
+        """Fix the launch shapes without measuring (fft_chunk 0: all planes)."""
+        check(lib().fhs_measop_set_tuning(self._h, int(fft_chunk), int(grid_slice)))
+
+    def tuning(self):
+        """The shapes in use and the autotuner's measurements (ms per candidate)."""
+        t = LB.Tuning()
+        check(lib().fhs_measop_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
     def set_preconditioner(self, pU):
         """Attach aW: ``pU[l]`` is one channel's preconditioner, either one
         array over its visibilities or a list over its blocks."""

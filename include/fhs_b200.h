@@ -183,6 +183,35 @@ FHS_API fhs_status fhs_measop_dr_cells(fhs_measop* op, int channel, int64_t* cel
  * FP32 precision of the device copy). */
 FHS_API fhs_status fhs_measop_dr_lambda(fhs_measop* op, int channel, double* lambda);
 
+/* Autotuner of the operator's launch shapes (no reference counterpart).
+ * Candidates, each timed on the operator itself with CUDA events (best of 3
+ * after a warm-up): planes per launch of the hand-written real-image FFT
+ * passes (all, 16, 8, 4: smaller chunks keep each pass's intermediate in L2
+ * for the next), and the most visibilities per gridding work item (8192,
+ * 16384, 32768, 65536: dense tiles split into more, shorter items).  The
+ * fastest of each is kept for every solver of the operator.  The first
+ * fhs_solver_init of an operator runs it unless fhs_measop_set_tuning fixed
+ * the shapes.  Split work items sum their partial tiles in another order, so
+ * different choices give results that differ at FP32 rounding level; fix the
+ * shapes for bit-reproducible runs. */
+#define FHS_TUNING_MAX_CANDIDATES 8
+typedef struct fhs_tuning {
+  int tuned;               /* 1 after fhs_measop_autotune or fhs_measop_set_tuning */
+  int fft_chunk;           /* planes per FFT launch (0: all planes; -1: library FFT, not tuned) */
+  int grid_slice;          /* visibilities per gridding work item (0: DR operator, not tuned) */
+  int n_fft, n_grid;       /* candidates measured (0 when fixed by fhs_measop_set_tuning) */
+  int fft_candidates[FHS_TUNING_MAX_CANDIDATES];
+  double fft_ms[FHS_TUNING_MAX_CANDIDATES];    /* forward + adjoint transforms, all planes */
+  int grid_candidates[FHS_TUNING_MAX_CANDIDATES];
+  double grid_ms[FHS_TUNING_MAX_CANDIDATES];   /* whole-operator gridding */
+} fhs_tuning;
+/* Measure the candidates now and keep the fastest (out may be NULL). */
+FHS_API fhs_status fhs_measop_autotune(fhs_measop* op, fhs_tuning* out);
+/* Fix the shapes without measuring: fft_chunk >= 0 (0: all planes),
+ * grid_slice >= 1024; solvers of op re-capture their iteration graph. */
+FHS_API fhs_status fhs_measop_set_tuning(fhs_measop* op, int fft_chunk, int grid_slice);
+FHS_API fhs_status fhs_measop_tuning(const fhs_measop* op, fhs_tuning* out);
+
 /* ======================================================================
  * Priors (standalone, device selected per call)
  * ====================================================================== */

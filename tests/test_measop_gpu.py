@@ -96,3 +96,27 @@ def test_compute_residual_images_matches_oracle():
     res = compute_residual_images(np.moveaxis(xk, 0, 2), data.y, op)
     ref = so.compute_residual_images(xk, data)
     assert rel(np.moveaxis(res, 2, 0), ref) < OP_TOL * 10
+
+
+@pytest.mark.parametrize("Ny,Nx,L,M", [(32, 32, 2, 600), (64, 128, 2, 3000), (256, 128, 3, 8000),
+                                       (512, 512, 2, 20000), (1024, 1024, 1, 40000), (2048, 2048, 1, 40000),
+                                       (32, 2048, 1, 4000), (2048, 32, 1, 4000)])
+def test_real_image_transforms_on_power_of_two_grids(Ny, Nx, L, M):
+    """Phi x and Re(Phi^H y) of real images through the hand-written FFTs
+    (every power-of-two grid side 64..4096, both axes, square and not)."""
+    from fhs_b200 import HS_adjoint_operator_G, HS_forward_operator_G
+    gop, ref, Gs = _make(Ny, Nx, L, M, 2, 41)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((Ny, Nx, L))
+    y = HS_forward_operator_G(x, gop)
+    for l in range(L):
+        assert rel(np.concatenate(y[l]), Gs[l] @ ref.A(x[:, :, l])) < OP_TOL
+    yr = [[rng.standard_normal(len(b)) + 1j * rng.standard_normal(len(b)) for b in yl] for yl in y]
+    xa = HS_adjoint_operator_G(yr, gop)
+    for l in range(L):
+        xo = np.real(ref.At(Gs[l].conj().T @ np.concatenate(yr[l])))
+        assert rel(xa[:, :, l], xo) < OP_TOL
+    # relative to ||x|| ||Phi^H y|| (the Cauchy-Schwarz bound of both sides):
+    # the sums cancel heavily for random vectors
+    lhs = sum(np.vdot(np.concatenate(yr[l]), np.concatenate(y[l])) for l in range(L)).real
+    assert abs(lhs - float(np.sum(xa * x))) / (np.linalg.norm(x) * np.linalg.norm(xa)) < ADJ_TOL
