@@ -25,10 +25,12 @@
 // thread straight from global memory into registers (no staging pass); the
 // other stages exchange through shared memory with a 1-in-8 padded layout
 // (conflict-free strided stores).  A butterfly reads one twiddle w from an
-// FP64-derived table and forms w^2..w^7 by products.  In the strided passes
-// the 4 lines of a CTA are interleaved across neighbouring threads, so four
-// threads read one 32-byte row segment.  FP32 arithmetic, unnormalised (the
-// adjoint of the forward transform), as the reference's fft2 / its adjoint.
+// FP64-derived table and forms w^2..w^7 by products.  The lines of a CTA are
+// interleaved across neighbouring threads (in the strided passes four
+// threads read one 32-byte row segment) with line starts placed so that
+// every shared-memory pass is free of bank conflicts.  FP32 arithmetic,
+// unnormalised (the adjoint of the forward transform), as the reference's
+// fft2 / its adjoint.
 #include "measop.cuh"
 
 #include <cmath>
@@ -206,10 +208,17 @@ __device__ __forceinline__ int image_index(int k, int n, int K) {
   return k < h ? k + h : (k >= K - h ? k - K + h : -1);
 }
 
-// padded line lengths: contiguous passes, and the interleaved strided passes
-// (line starts 16 banks apart)
-constexpr int line_len(int N) { return N + N / 8; }
-constexpr int strided_len(int N) { return N + N / 8 + (((N / 4) % 32 == 0) ? 8 : 0); }
+// Shared-memory layout of the LPC lines of a CTA.  Lines are interleaved
+// across threads (thread t: line t mod LPC, butterfly index t / LPC), so a
+// half-warp -- the unit of a 64-bit shared access -- holds 16 / LPC
+// consecutive elements of each of its LPC lines, which lie inside one padding
+// group of 8.  Line starts 16 / LPC slots (of 8 bytes) apart modulo 16 give
+// each line of the half-warp its own banks: one wavefront per half-warp for
+// the consecutive reads and writes of every stage and for the first stage's
+// stores at 9 j + r.
+constexpr int line_len(int N, int LPC) {
+  return N + N / 8 + ((16 / LPC - (N + N / 8) % 16) % 16 + 16) % 16;
+}
 
 // F1: x[L][Nx][Ny] (scaled by sy, sx) -> columns of the half spectrum; LPC
 // lines (column pairs) per CTA, TL threads each
@@ -219,8 +228,8 @@ __global__ void __launch_bounds__((1 << LOGN) / (8 * GM) * LPC) fft_f1_kernel(
     const float2* __restrict__ tw, int Ny, int Nx, int Kx, int p0, float2* __restrict__ half) {
   constexpr int N = 1 << LOGN, TL = N / (8 * GM), Kh = N / 2 + 1;
   extern __shared__ float2 f1_sm[];
-  const int line = threadIdx.x / TL, tl = threadIdx.x - line * TL;
-  float2* buf = f1_sm + line * line_len(N);
+  const int line = threadIdx.x % LPC, tl = threadIdx.x / LPC;
+  float2* buf = f1_sm + line * line_len(N, LPC);
   const int pair = blockIdx.x * LPC + line;
   const bool active = pair < Nx / 2;
   const int ia = 2 * (active ? pair : 0), ib = ia + 1;
@@ -254,7 +263,7 @@ __global__ void __launch_bounds__((1 << LOGN) / (8 * GM) * kFftLines, GM <= 2 ? 
   constexpr int N = 1 << LOGN, TL = N / (8 * GM);
   extern __shared__ float2 f2_sm[];
   const int b = threadIdx.x & (kFftLines - 1), tl = threadIdx.x / kFftLines;
-  float2* buf = f2_sm + b * strided_len(N);
+  float2* buf = f2_sm + b * line_len(N, kFftLines);
   const int Kh = Ky / 2 + 1;
   const int row = blockIdx.x * kFftLines + b;
   const bool valid = row < Kh;
@@ -275,7 +284,7 @@ __global__ void __launch_bounds__((1 << LOGN) / (8 * GM) * kFftLines, GM <= 2 ? 
   constexpr int N = 1 << LOGN, TL = N / (8 * GM);
   extern __shared__ float2 i1_sm[];
   const int b = threadIdx.x & (kFftLines - 1), tl = threadIdx.x / kFftLines;
-  float2* buf = i1_sm + b * strided_len(N);
+  float2* buf = i1_sm + b * line_len(N, kFftLines);
   const int Kh = Ky / 2 + 1;
   const int plane = p0 + blockIdx.y;
   const int ky0 = blockIdx.x * kFftLines + b;
@@ -304,8 +313,8 @@ __global__ void __launch_bounds__((1 << LOGN) / (8 * GM) * LPC) fft_i2_kernel(
     const float2* __restrict__ tw, const float2* __restrict__ U, int Ny, int Nx, int p0, float* __restrict__ out) {
   constexpr int N = 1 << LOGN, TL = N / (8 * GM), Kh = N / 2 + 1;
   extern __shared__ float2 i2_sm[];
-  const int line = threadIdx.x / TL, tl = threadIdx.x - line * TL;
-  float2* buf = i2_sm + line * line_len(N);
+  const int line = threadIdx.x % LPC, tl = threadIdx.x / LPC;
+  float2* buf = i2_sm + line * line_len(N, LPC);
   const int pair = blockIdx.x * LPC + line;
   const bool active = pair < Nx / 2;
   const int ia = 2 * (active ? pair : 0), ib = ia + 1;
@@ -342,18 +351,18 @@ int log2i(int n) {
 }
 
 // launch shapes: contiguous passes (F1, I2) use TL = min(N / 8, 256) threads
-// per line and LPC lines per CTA (at least 128 threads); strided passes (F2,
-// I1) use 4 lines of TL = min(N / 8, 128) threads
+// per line and LPC >= 2 lines per CTA (at least 128 threads); strided passes
+// (F2, I1) use 4 lines of TL = min(N / 8, 128) threads
 template <int LOGN>
 struct Shape {
   static constexpr int N = 1 << LOGN;
   static constexpr int GMc = N > 2048 ? 2 : 1;
   static constexpr int TLc = N / (8 * GMc);
-  static constexpr int LPC = TLc >= 128 ? 1 : 128 / TLc;
+  static constexpr int LPC = TLc >= 64 ? 2 : 128 / TLc;
   static constexpr int GMs = N > 1024 ? N / 1024 : 1;
   static constexpr int TLs = N / (8 * GMs);
-  static constexpr size_t smem_c = (size_t)LPC * line_len(N) * sizeof(float2);
-  static constexpr size_t smem_s = (size_t)kFftLines * strided_len(N) * sizeof(float2);
+  static constexpr size_t smem_c = (size_t)LPC * line_len(N, LPC) * sizeof(float2);
+  static constexpr size_t smem_s = (size_t)kFftLines * line_len(N, kFftLines) * sizeof(float2);
 };
 
 template <int LOGN>
