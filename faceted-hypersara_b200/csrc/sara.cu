@@ -248,8 +248,9 @@ __device__ __forceinline__ void analysis_prox_body(const LevelArgs& a, int b, in
   const size_t mm = (size_t)m0 * m1;
   constexpr int NSUB = LAST ? 4 : 3;
   const int64_t off[4] = {a.h_off[b], a.h_off[b] + (int64_t)mm, a.h_off[b] + 2 * (int64_t)mm, a.a_off[b]};
-  const float* lo_f = c_lo[b];  // uniform per CTA: constant-cache broadcast
-  const float* hi_f = c_hi[b];
+  // the basis is LF / 2 - 1: the taps are compile-time constant-bank operands
+  const float* lo_f = c_lo[LF / 2 - 1];
+  const float* hi_f = c_hi[LF / 2 - 1];
   float w[NSUB][MAXL];
 #pragma unroll
   for (int l = 0; l < MAXL; ++l) {
@@ -266,17 +267,26 @@ __device__ __forceinline__ void analysis_prox_body(const LevelArgs& a, int b, in
     const int nch = min(CH, lg - c0);
     if (nch <= 0) continue;
     // ---- step 1: x filtering of (row, channel) tasks
+    // (interior tiles read their whole input window without bounds tests)
+    const bool inside = i0s >= 0 && i0s + IN0 <= n0 && i1s >= 0 && i1s + IN1 <= n1;
+    const float scale = a.in_scale;
     for (int task = threadIdx.x; task < IN0 * nch; task += blockDim.x) {
       const int r = task % IN0, lc = task / IN0;
       const size_t plane = (size_t)g * lg + c0 + lc;
       const float* src = a.first ? x + plane * a.in_stride : apx + plane * a.apx_stride + a.in_off[b];
       const int i0 = i0s + r;
       float v[IN1];
-      const bool rin = i0 >= 0 && i0 < n0;
+      if (inside) {
+        const float* row = src + (ptrdiff_t)i1s * n0 + i0;
 #pragma unroll
-      for (int c = 0; c < IN1; ++c) {
-        const int i1 = i1s + c;
-        v[c] = (rin && i1 >= 0 && i1 < n1) ? src[(size_t)i1 * n0 + i0] * a.in_scale : 0.f;
+        for (int c = 0; c < IN1; ++c) v[c] = row[c * n0];
+      } else {
+        const bool rin = i0 >= 0 && i0 < n0;
+#pragma unroll
+        for (int c = 0; c < IN1; ++c) {
+          const int i1 = i1s + c;
+          v[c] = (rin && i1 >= 0 && i1 < n1) ? src[(size_t)i1 * n0 + i0] : 0.f;
+        }
       }
       float* base = sm + (size_t)lc * 4 * AT1 * APH;
       const int par = r & 1, rh = r >> 1;
@@ -288,12 +298,49 @@ __device__ __forceinline__ void analysis_prox_body(const LevelArgs& a, int b, in
           lo = fmaf(lo_f[t], v[2 * q + LF - 1 - t], lo);
           hi = fmaf(hi_f[t], v[2 * q + LF - 1 - t], hi);
         }
-        base[(0 + par) * AT1 * APH + q * APH + rh] = lo;
-        base[(2 + par) * AT1 * APH + q * APH + rh] = hi;
+        base[(0 + par) * AT1 * APH + q * APH + rh] = lo * scale;
+        base[(2 + par) * AT1 * APH + q * APH + rh] = hi * scale;
       }
     }
     __syncthreads();
     // ---- step 2: y filtering by the owner of each coefficient
+    if constexpr (MAXL <= kApChunk) {
+      // channels unrolled inside the taps: the filter sums accumulate straight
+      // into the dual w[][l] (compile-time register indices, no selects)
+      float aa[LAST ? 1 : MAXL];
+#pragma unroll
+      for (int l = 0; l < (LAST ? 1 : MAXL); ++l) aa[l] = 0.f;
+      const float* col = sm + lp1 * APH;
+#pragma unroll
+      for (int t = 0; t < LF; ++t) {
+        const int r = 2 * lp0 + LF - 1 - t;   // parity of r is that of LF - 1 - t
+        const int par = (LF - 1 - t) & 1, rh = r >> 1;
+#pragma unroll
+        for (int l = 0; l < MAXL; ++l) {
+          if (l < nch) {
+            const float* base = col + (size_t)l * 4 * AT1 * APH;
+            const float lo = base[(0 + par) * AT1 * APH + rh];
+            const float hi = base[(2 + par) * AT1 * APH + rh];
+            w[0][l] = fmaf(hi_f[t], lo, w[0][l]);
+            w[1][l] = fmaf(lo_f[t], hi, w[1][l]);
+            w[2][l] = fmaf(hi_f[t], hi, w[2][l]);
+            if constexpr (LAST)
+              w[NSUB - 1][l] = fmaf(lo_f[t], lo, w[NSUB - 1][l]);
+            else
+              aa[l] = fmaf(lo_f[t], lo, aa[l]);
+          }
+        }
+      }
+      if constexpr (!LAST) {
+        if (valid) {
+#pragma unroll
+          for (int l = 0; l < MAXL; ++l)
+            if (l < nch) apx[((size_t)g * lg + l) * a.apx_stride + a.a_off[b] + o] = aa[l];
+        }
+      }
+      __syncthreads();
+      continue;
+    }
 #pragma unroll 1
     for (int lc = 0; lc < CH; ++lc) {
       const int l = c0 + lc;
