@@ -1,10 +1,9 @@
 // Allocation-free l2-ball projection (device pointers, static scratch).
 //
-// Callers that must not allocate device memory use this entry point: code
-// that runs inside a CUDA stream capture (an allocation there breaks or
-// serialises the capture), host frameworks that own the whole device heap
-// through their own pool (MATLAB gpuArray, PyTorch's caching allocator) and
-// real-time pipelines that forbid allocation after start-up.  The caller
+// Callers that must not allocate device memory use this entry point: host
+// frameworks that own the whole device heap through their own pool (MATLAB
+// gpuArray, PyTorch's caching allocator) and real-time pipelines that forbid
+// allocation after start-up.  The caller
 // passes device buffers for the inputs and the output; the partial sums of
 // ||x - y||^2 live in a file-scope device array that every call on a device
 // shares.

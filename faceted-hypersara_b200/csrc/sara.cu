@@ -454,6 +454,203 @@ void launch_analysis_prox(dim3 grid, cudaStream_t s, const LevelArgs& a, const f
   analysis_prox_kernel<MAXL><<<grid, 256, smem, s>>>(a, x, apx, v1, weights, beta, lg, l21_acc);
 }
 
+// The same fused level for groups of at most 16 channels with two threads per
+// coefficient position (512 threads per 32 x 8 tile): thread branch 0 takes
+// the y-low-pass of the x-low rows (A) and their y-high-pass (H), branch 1
+// the y-low and y-high passes of the x-high rows (V, D).  Each thread holds
+// 2 subbands x 16 channels of the dual, loaded after the x filtering, so the
+// kernel fits 64 registers and 2 CTAs per SM (32 warps).
+constexpr int kApSplitThreads = 2 * AT0 * AT1;
+
+// step 1 of the split kernel: (input row, channel) tasks filter and
+// downsample along x (all 512 threads) into sm [channel][lo e/o, hi e/o][AT1][APH]
+template <int LF>
+__device__ __forceinline__ void ap_split_xfilter(const LevelArgs& a, int b, int tile, int g,
+                                                 const float* __restrict__ x, const float* __restrict__ apx, int lg,
+                                                 float* sm) {
+  constexpr int IN0 = 2 * AT0 + LF - 2, IN1 = 2 * AT1 + LF - 2;
+  constexpr int B = LF / 2 - 1;
+  static_assert(IN0 <= 2 * APH, "row buffer too small");
+  const float* lo_f = c_lo[B];
+  const float* hi_f = c_hi[B];
+  const int n0 = a.n0[b], n1 = a.n1[b];
+  const int tp0 = tile % a.tiles0[b], tp1 = tile / a.tiles0[b];
+  const int i0s = 2 * tp0 * AT0 + 2 - LF, i1s = 2 * tp1 * AT1 + 2 - LF;
+  const bool inside = i0s >= 0 && i0s + IN0 <= n0 && i1s >= 0 && i1s + IN1 <= n1;
+  const float scale = a.in_scale;
+  for (int task = threadIdx.x; task < IN0 * lg; task += kApSplitThreads) {
+    const int r = task % IN0, lc = task / IN0;
+    const size_t plane = (size_t)g * lg + lc;
+    const float* src = a.first ? x + plane * a.in_stride : apx + plane * a.apx_stride + a.in_off[b];
+    const int i0 = i0s + r;
+    float v[IN1];
+    if (inside) {
+      const float* row = src + (ptrdiff_t)i1s * n0 + i0;
+#pragma unroll
+      for (int c = 0; c < IN1; ++c) v[c] = row[c * n0];
+    } else {
+      const bool rin = i0 >= 0 && i0 < n0;
+#pragma unroll
+      for (int c = 0; c < IN1; ++c) {
+        const int i1 = i1s + c;
+        v[c] = (rin && i1 >= 0 && i1 < n1) ? src[(size_t)i1 * n0 + i0] : 0.f;
+      }
+    }
+    float* base = sm + (size_t)lc * 4 * AT1 * APH;
+    const int par = r & 1, rh = r >> 1;
+#pragma unroll
+    for (int q = 0; q < AT1; ++q) {
+      float lo = 0.f, hi = 0.f;
+#pragma unroll
+      for (int t = 0; t < LF; ++t) {
+        lo = fmaf(lo_f[t], v[2 * q + LF - 1 - t], lo);
+        hi = fmaf(hi_f[t], v[2 * q + LF - 1 - t], hi);
+      }
+      base[(0 + par) * AT1 * APH + q * APH + rh] = lo * scale;
+      base[(2 + par) * AT1 * APH + q * APH + rh] = hi * scale;
+    }
+  }
+}
+
+// steps 2-3 of the split kernel for branch BR: the dual of the branch's two
+// subbands, the y filtering accumulated into it, the weighted l21 prox
+template <int MAXL, int LF, bool LAST, int BR>
+__device__ __forceinline__ void ap_split_tail(const LevelArgs& a, int b, int tile, int g, float* __restrict__ apx,
+                                              float* __restrict__ v1, const float* __restrict__ weights,
+                                              const double* __restrict__ beta, int lg,
+                                              double* __restrict__ l21_acc, const float* sm, double* red) {
+  constexpr int B = LF / 2 - 1;
+  static_assert(MAXL <= kApChunk, "one staging round");
+  // the two y filters of this branch: f0 -> subband k0, f1 -> subband k1
+  // (branch 0: H = hi(y) lo(x), A = lo(y) lo(x); branch 1: V = lo(y) hi(x), D = hi(y) hi(x))
+  const float* f0 = BR == 0 ? c_hi[B] : c_lo[B];
+  const float* f1 = BR == 0 ? c_lo[B] : c_hi[B];
+  const int m0 = a.m0[b], m1 = a.m1[b];
+  const int tp0 = tile % a.tiles0[b], tp1 = tile / a.tiles0[b];
+  const int pos = threadIdx.x % (AT0 * AT1);
+  const int lp0 = pos % AT0, lp1 = pos / AT0;
+  const int p0 = tp0 * AT0 + lp0, p1 = tp1 * AT1 + lp1;
+  const bool valid = p0 < m0 && p1 < m1;
+  const size_t o = (size_t)p1 * m0 + p0;
+  const size_t mm = (size_t)m0 * m1;
+  // subbands of this branch in the coefficient vector: H, V, D at h_off + k mm, A at a_off
+  const int64_t off0 = a.h_off[b] + (BR == 0 ? 0 : (int64_t)mm);
+  const int64_t off1 = BR == 0 ? a.a_off[b] : a.h_off[b] + 2 * (int64_t)mm;
+  constexpr bool PROX1 = BR == 1 || LAST;   // A is a prox subband only at the last level
+  const int nch = lg;
+  float w0[MAXL], w1[MAXL];
+#pragma unroll
+  for (int l = 0; l < MAXL; ++l) {
+    w0[l] = 0.f;
+    w1[l] = 0.f;
+    if (l < nch && valid) {
+      const float* vp = v1 + ((size_t)g * lg + l) * a.s_stride + o;
+      w0[l] = vp[off0];
+      if (PROX1) w1[l] = vp[off1];
+    }
+  }
+  __syncthreads();   // step 1 complete
+  // taps in pairs (2u, 2u + 1): rows 2 lp0 + LF - 1 - t of odd then even
+  // parity share the half-row index lp0 + LF / 2 - 1 - u; the pair loop is
+  // not unrolled (compact code: all bases and branches of a launch share the
+  // instruction cache), the channels are
+  const float* col = sm + (BR == 0 ? 0 : 2) * AT1 * APH + lp1 * APH + lp0 + LF / 2 - 1;
+#pragma unroll 1
+  for (int u = 0; u < LF / 2; ++u) {
+    const float f0o = f0[2 * u], f0e = f0[2 * u + 1], f1o = f1[2 * u], f1e = f1[2 * u + 1];
+    const float* cu = col - u;
+#pragma unroll
+    for (int l = 0; l < MAXL; ++l) {
+      if (l < nch) {
+        const float so = cu[(size_t)l * 4 * AT1 * APH + AT1 * APH];   // odd rows
+        const float se = cu[(size_t)l * 4 * AT1 * APH];               // even rows
+        w0[l] = fmaf(f0o, so, fmaf(f0e, se, w0[l]));
+        w1[l] = fmaf(f1o, so, fmaf(f1e, se, w1[l]));
+      }
+    }
+  }
+  if (!PROX1 && valid) {   // coarser level: A goes to the approximation scratch
+#pragma unroll
+    for (int l = 0; l < MAXL; ++l)
+      if (l < nch) apx[((size_t)g * lg + l) * a.apx_stride + a.a_off[b] + o] = w1[l];
+  }
+  double l21 = 0.0;
+  if (valid) {
+    const float bt = (float)beta[g];
+    const float* wg = weights + (size_t)g * a.s_stride + o;
+    auto prox = [&](float(&w)[MAXL], int64_t off) {
+      float ss = 0.f;
+#pragma unroll
+      for (int l = 0; l < MAXL; ++l)
+        if (l < nch) ss = fmaf(w[l], w[l], ss);
+      const float l2 = sqrtf(ss);
+      l21 += l2;
+      const float soft = fmaxf(l2 - bt * wg[off], 0.f) / (l2 + 2.220446049250313e-16f);
+      float* dst = v1 + (size_t)g * lg * a.s_stride + off + o;
+#pragma unroll
+      for (int l = 0; l < MAXL; ++l)
+        if (l < nch) dst[(size_t)l * a.s_stride] = w[l] - soft * w[l];
+    };
+    prox(w0, off0);
+    if (PROX1) prox(w1, off1);
+  }
+  if (l21_acc) {
+    for (int sh = 16; sh > 0; sh >>= 1) l21 += __shfl_down_sync(0xffffffffu, l21, sh);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l21;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int i = 0; i < kApSplitThreads / 32; ++i) t += red[i];
+      atomicAdd(l21_acc + g, t);
+    }
+  }
+}
+
+template <int MAXL>
+__global__ void __launch_bounds__(kApSplitThreads, 2) analysis_prox_split_kernel(
+    LevelArgs a, const float* __restrict__ x, float* __restrict__ apx, float* __restrict__ v1,
+    const float* __restrict__ weights, const double* __restrict__ beta, int lg, double* __restrict__ l21_acc) {
+  extern __shared__ float sm_ap[];
+  __shared__ double red[kApSplitThreads / 32];
+  const int band = blockIdx.x / (kSaraWavelets * kApBand);
+  const int rem = blockIdx.x - band * (kSaraWavelets * kApBand);
+  const int b = rem / kApBand, tile = band * kApBand + rem % kApBand, g = blockIdx.y;
+  if (tile >= a.tiles[b]) return;
+  const int br = threadIdx.x / (AT0 * AT1);   // warp-uniform
+#define FHS_C(BB, LFV)                                                                                  \
+  case BB:                                                                                              \
+    ap_split_xfilter<LFV>(a, b, tile, g, x, apx, lg, sm_ap);                                            \
+    if (a.last) {                                                                                       \
+      if (br == 0)                                                                                      \
+        ap_split_tail<MAXL, LFV, true, 0>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red);  \
+      else                                                                                              \
+        ap_split_tail<MAXL, LFV, true, 1>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red);  \
+    } else {                                                                                            \
+      if (br == 0)                                                                                      \
+        ap_split_tail<MAXL, LFV, false, 0>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); \
+      else                                                                                              \
+        ap_split_tail<MAXL, LFV, false, 1>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); \
+    }                                                                                                   \
+    break;
+  switch (b) { FHS_C(0, 2) FHS_C(1, 4) FHS_C(2, 6) FHS_C(3, 8) FHS_C(4, 10) FHS_C(5, 12) FHS_C(6, 14) FHS_C(7, 16) }
+#undef FHS_C
+}
+
+template <int MAXL>
+void launch_analysis_prox_split(dim3 grid, cudaStream_t s, const LevelArgs& a, const float* x, float* apx,
+                                float* v1, const float* weights, const double* beta, int lg, double* l21_acc) {
+  const size_t smem = analysis_prox_smem<MAXL>();
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (smem > 48 * 1024 && dev < 64 && !attr[dev]) {
+    FHS_CUDA(cudaFuncSetAttribute(analysis_prox_split_kernel<MAXL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    attr[dev] = true;
+  }
+  analysis_prox_split_kernel<MAXL><<<grid, kApSplitThreads, smem, s>>>(a, x, apx, v1, weights, beta, lg, l21_acc);
+}
+
 // ----------------------------------------------------------- synthesis
 // One synthesis level is the adjoint of an analysis level: with an even tile
 // start, the output pair (2k, 2k+1) along an axis draws on the same LF/2
@@ -541,21 +738,30 @@ __device__ __forceinline__ void syn_basis(int b, SynSmem& S, int buf, float acc[
     lo[t] = c_lo[b][t];
     hi[t] = c_hi[b][t];
   }
-  // along y: task = (column l1, output pair k), k fastest
-  for (int task = threadIdx.x; task < RX * (SY / 2); task += blockDim.x) {
-    const int l1 = task / (SY / 2), k = task - l1 * (SY / 2);
-    float le = 0.f, lo_ = 0.f, he = 0.f, ho = 0.f;
+  // along y: task = (column l1, output pairs k, k + 1), k even and fastest;
+  // the two pairs share H - 1 of their H + 1 coefficient rows
+  for (int task = threadIdx.x; task < RX * (SY / 4); task += blockDim.x) {
+    const int l1 = task / (SY / 4), k = 2 * (task - l1 * (SY / 4));
+    float le0 = 0.f, lo0 = 0.f, he0 = 0.f, ho0 = 0.f, le1 = 0.f, lo1 = 0.f, he1 = 0.f, ho1 = 0.f;
 #pragma unroll
-    for (int j = 0; j < H; ++j) {
+    for (int j = 0; j <= H; ++j) {
       const float ca = S.sub[buf][0][l1][k + j], ch = S.sub[buf][1][l1][k + j];
       const float cv = S.sub[buf][2][l1][k + j], cd = S.sub[buf][3][l1][k + j];
-      le = fmaf(ca, lo[2 * j + 1], fmaf(ch, hi[2 * j + 1], le));
-      lo_ = fmaf(ca, lo[2 * j], fmaf(ch, hi[2 * j], lo_));
-      he = fmaf(cv, lo[2 * j + 1], fmaf(cd, hi[2 * j + 1], he));
-      ho = fmaf(cv, lo[2 * j], fmaf(cd, hi[2 * j], ho));
+      if (j < H) {   // tap j of pair k
+        le0 = fmaf(ca, lo[2 * j + 1], fmaf(ch, hi[2 * j + 1], le0));
+        lo0 = fmaf(ca, lo[2 * j], fmaf(ch, hi[2 * j], lo0));
+        he0 = fmaf(cv, lo[2 * j + 1], fmaf(cd, hi[2 * j + 1], he0));
+        ho0 = fmaf(cv, lo[2 * j], fmaf(cd, hi[2 * j], ho0));
+      }
+      if (j > 0) {   // tap j - 1 of pair k + 1
+        le1 = fmaf(ca, lo[2 * j - 1], fmaf(ch, hi[2 * j - 1], le1));
+        lo1 = fmaf(ca, lo[2 * j - 2], fmaf(ch, hi[2 * j - 2], lo1));
+        he1 = fmaf(cv, lo[2 * j - 1], fmaf(cd, hi[2 * j - 1], he1));
+        ho1 = fmaf(cv, lo[2 * j - 2], fmaf(cd, hi[2 * j - 2], ho1));
+      }
     }
-    *reinterpret_cast<float2*>(&S.tl[l1][2 * k]) = make_float2(le, lo_);
-    *reinterpret_cast<float2*>(&S.th[l1][2 * k]) = make_float2(he, ho);
+    *reinterpret_cast<float4*>(&S.tl[l1][2 * k]) = make_float4(le0, lo0, le1, lo1);
+    *reinterpret_cast<float4*>(&S.th[l1][2 * k]) = make_float4(he0, ho0, he1, ho1);
   }
   __syncthreads();
   // along x: output row i0, pairs m = 4 grp + q (columns 2m, 2m+1)
@@ -596,7 +802,7 @@ __device__ __forceinline__ void syn_dispatch(int b, SynSmem& S, int buf, float a
 // Buffer (b+1)&1 was last read by basis b-1's y pass, which every thread has
 // finished at basis b-1's second barrier; tl/th are rewritten by basis b's y
 // pass only after its first barrier, which follows basis b-1's x pass.
-__global__ void __launch_bounds__(256) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
+__global__ void __launch_bounds__(256, 4) synthesis_kernel(SynArgs a, const float* __restrict__ coef,
                                                         float* __restrict__ apx, float* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char syn_smem[];
   SynSmem& S = *reinterpret_cast<SynSmem*>(syn_smem);
@@ -828,13 +1034,13 @@ void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* 
     dim3 grid(ceil_div(maxt, kApBand) * kSaraWavelets * kApBand, n_groups);
 #define FHS_AP(MAXL) launch_analysis_prox<MAXL>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc)
     if (lg <= 1)
-      FHS_AP(1);
+      launch_analysis_prox_split<1>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc);
     else if (lg <= 4)
-      FHS_AP(4);
+      launch_analysis_prox_split<4>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc);
     else if (lg <= 8)
-      FHS_AP(8);
+      launch_analysis_prox_split<8>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc);
     else if (lg <= 16)
-      FHS_AP(16);
+      launch_analysis_prox_split<16>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc);
     else
       FHS_AP(32);
 #undef FHS_AP

@@ -219,10 +219,9 @@ FHS_API fhs_status fhs_measop_tuning(const fhs_measop* op, fhs_tuning* out);
 FHS_API fhs_status fhs_proj_l2ball(int device, int64_t n, const double* x, double eps, const double* y,
                            double* p);
 /* Allocation-free variant of fhs_proj_l2ball (no counterpart in the
- * reference).  For callers that cannot allocate device memory: code inside a
- * CUDA stream capture, hosts whose own pool owns the device heap (MATLAB
- * gpuArray, PyTorch's caching allocator), real-time pipelines that forbid
- * allocation after start-up.  x, y, p are DEVICE pointers to n interleaved
+ * reference).  For callers that cannot allocate device memory: hosts whose
+ * own pool owns the device heap (MATLAB gpuArray, PyTorch's caching
+ * allocator), real-time pipelines that forbid allocation after start-up.  x, y, p are DEVICE pointers to n interleaved
  * complex doubles; the call is enqueued on `stream` (a cudaStream_t, NULL =
  * legacy default stream) and returns without synchronising.  Scratch: a
  * 512 KB static device array per device that every call shares; n is limited

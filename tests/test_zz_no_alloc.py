@@ -1,8 +1,8 @@
 """The allocation-free l2-ball projection (fhs_proj_l2ball_noalloc).
 
-Some callers cannot allocate device memory (code inside a CUDA stream
-capture, hosts whose own pool owns the device heap, real-time pipelines that
-forbid allocation after start-up); this entry point takes device buffers and
+Some callers cannot allocate device memory (hosts whose own pool owns the
+device heap, real-time pipelines that forbid allocation after start-up); this
+entry point takes device buffers and
 keeps its partial sums in a static device array.  The test calls it through
 the C ABI twice in a row, with different sizes and inputs, and checks each
 result against fhs_proj_l2ball (the allocating entry point) to the 1e-12
