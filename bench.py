@@ -190,9 +190,23 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of a
 # stage at the bench workload, from one ncu capture of the current kernels
 # (the medium case, 512 x 512 x 64, scaled by 4: grid cells, visibilities,
-# pixels and coefficients all grow by 4 to 1024 x 1024 x 64).  A stage
+# pixels and coefficients all grow by 4 to 1024 x 1024 x 64), summed over the
+# stage's launches in one iteration (ncu --metrics
+# gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum).  A stage
 # without a capture of its current code reports traffic null.
-TRAFFIC_PER_LAUNCH = {}
+_MB = 1e6
+TRAFFIC_PER_LAUNCH = {
+    "grid_dual": 4 * (450 + 335) * _MB,
+    "sara_analysis_prox": 4 * (872 + 599 + 138 + 23) * _MB,
+    "sara_synthesis": 4 * (819 + 156) * _MB,
+    "degrid_dual": 4 * (691 + 157) * _MB,
+    "fft_inverse": 4 * (537 + 118 + 134 + 35) * _MB,
+    "fft_forward": 4 * (67 + 75 + 134 + 211) * _MB,
+    "assemble_g": 4 * (212 + 46) * _MB,
+    "facet_reconstruct": 4 * (148 + 30) * _MB,
+    "facet_gram": 4 * (145 + 1 + 1) * _MB,
+    "primal_pad": 4 * (134 + 75) * _MB,
+}
 
 
 def _cpu_sample(wl, seed=0):
