@@ -57,6 +57,28 @@ static float* img_scratch(MeasOp* op) {
   return op->img_a.p;
 }
 
+void measop_real_forward(const MeasOp* op, const float* img, float2* vis, cudaStream_t s) {
+  if (op->tw_y.p) {   // hand-written real-to-half-spectrum transforms
+    fft_forward_half(op, img, 0, op->L, s);
+    launch_degrid_plain(op, 0, op->L, vis, s, true);
+  } else {
+    launch_pad(op, img, 0, op->L, s);
+    fft_forward(op, 0, op->L, s);
+    launch_degrid_plain(op, 0, op->L, vis, s);
+  }
+}
+
+void measop_real_adjoint(const MeasOp* op, const float2* vis, float* img, cudaStream_t s) {
+  launch_grid_plain(op, 0, op->L, vis, s);
+  if (op->tw_y.p) {   // hand-written spectrum-to-real transforms
+    fft_inverse_real(op, img, 0, op->L, s);
+    launch_scale_image(op, img, op->L, s);
+  } else {
+    fft_inverse(op, 0, op->L, s);
+    launch_crop_real(op, img, nullptr, 0, op->L, s);
+  }
+}
+
 // HS_forward_operator_G.m:36-52 (precond: HS_forward_operator_precond_G.m:40-55,
 // y = sqrt(pU) .* G A x), all channels, host buffers.
 static void forward_impl(MeasOp* op, const double* x, double* y, bool precond) {
@@ -70,14 +92,7 @@ static void forward_impl(MeasOp* op, const double* x, double* y, bool precond) {
   float2* va = vis_scratch(op, op->vis_a);
   FHS_CUDA(cudaMemcpyAsync(st, x, N * op->L * sizeof(double), cudaMemcpyHostToDevice, s));
   launch_d2f(st, img, N * op->L, s);
-  if (op->tw_y.p) {   // hand-written real-to-half-spectrum transforms
-    fft_forward_half(op, img, 0, op->L, s);
-    launch_degrid_plain(op, 0, op->L, va, s, true);
-  } else {
-    launch_pad(op, img, 0, op->L, s);
-    fft_forward(op, 0, op->L, s);
-    launch_degrid_plain(op, 0, op->L, va, s);
-  }
+  measop_real_forward(op, img, va, s);
   if (precond) launch_scale_pu(op, va, true, s);
   launch_vis_scatter(va, st, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
   FHS_CUDA(cudaMemcpyAsync(y, st, 2 * op->Mtot * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -98,14 +113,7 @@ static void adjoint_impl(MeasOp* op, const double* y, double* x, bool precond) {
   FHS_CUDA(cudaMemcpyAsync(st, y, 2 * op->Mtot * sizeof(double), cudaMemcpyHostToDevice, s));
   launch_vis_gather(st, va, op->perm.p, op->ch_voff.p, op->ch_M.p, 0, op->L, op->maxM, 0, s);
   if (precond) launch_scale_pu(op, va, true, s);
-  launch_grid_plain(op, 0, op->L, va, s);
-  if (op->tw_y.p) {   // hand-written spectrum-to-real transforms
-    fft_inverse_real(op, img, 0, op->L, s);
-    launch_scale_image(op, img, op->L, s);
-  } else {
-    fft_inverse(op, 0, op->L, s);
-    launch_crop_real(op, img, nullptr, 0, op->L, s);
-  }
+  measop_real_adjoint(op, va, img, s);
   launch_f2d(img, st, N * op->L, s);
   FHS_CUDA(cudaMemcpyAsync(x, st, N * op->L * sizeof(double), cudaMemcpyDeviceToHost, s));
   FHS_CUDA(cudaStreamSynchronize(s));

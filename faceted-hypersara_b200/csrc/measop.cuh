@@ -228,6 +228,11 @@ void solver_fft_inverse(const MeasOp* op, cudaStream_t s);
 void launch_grid_plain(const MeasOp* op, int c0, int nc, const float2* v, cudaStream_t s);
 // out[l] = sigma[l] * s .* real(gridA cropped) (planes [p0, p0+np)); sigma NULL -> 1
 void launch_crop_real(const MeasOp* op, float* out, const float* sigma, int p0, int np, cudaStream_t s);
+// Phi x of real images x[L][Nx][Ny] (all channels) into vis (sorted order),
+// and Re(Phi^H v) back into img[L][Nx][Ny]: the API-level forward / adjoint
+// (hand-written FFTs when the grid sides allow them)
+void measop_real_forward(const MeasOp* op, const float* img, float2* vis, cudaStream_t s);
+void measop_real_adjoint(const MeasOp* op, const float2* vis, float* img, cudaStream_t s);
 // img[p] *= s (the min-max scaling factors sy[iy] sx[ix]), planes [0, np) of a compact [np][Nx][Ny] image
 void launch_scale_image(const MeasOp* op, float* img, int np, cudaStream_t s);
 // fused dual update, pass 1: GFx, z = v2 + 2 GFx - gold - y -> zbuf, GFx -> gold, block partials

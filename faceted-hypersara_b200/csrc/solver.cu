@@ -628,51 +628,62 @@ fhs_status fhs_solver_set_params(fhs_solver* s_, const fhs_solver_params* p) {
   });
 }
 
+}  // extern "C"
+
+namespace fhs {
+
+void solver_init_state(Solver* S, const double* xinit, const float* xinit_dev) {
+  FHS_CHECK(S->params_set && S->data_set, FHS_ERR_STATE, "set data and params before init");
+  MeasOp* op = S->op;
+  DeviceGuard dg(op->device);
+  cudaStream_t s = op->stream;
+  if (!op->tuned) measop_autotune(op);   // before any state: the timed launches use scratch only
+  const int64_t n = (int64_t)S->L * S->N;
+  if (xinit) {
+    if (op->stage.n < (size_t)n) op->stage.alloc(n);
+    FHS_CUDA(cudaMemcpyAsync(op->stage.p, xinit, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_d2f(op->stage.p, S->x.p, n, s);
+  } else if (xinit_dev) {
+    FHS_CUDA(cudaMemcpyAsync(S->x.p, xinit_dev, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  } else {
+    S->x.zero(s);
+  }
+  S->g.zero(s);
+  S->v1.zero(s);
+  S->v2.zero(s);
+  S->g1.zero(s);
+  if (S->nuclear) S->v0.zero(s);
+  S->ring_counter.zero(s);
+  // Fx_old: keep G A x_init per visibility (linearity of G)
+  if (!op->own_fft) launch_pad_real(op, S->x.p, 0, S->L, s);
+  solver_fft_forward(op, S->x.p, s);
+  launch_degrid_plain(op, 0, S->L, S->gold.p, s, true);
+  S->precond = op->precond;
+  if (S->precond) {
+    if (S->projw.n < (size_t)std::max<int64_t>(op->Mtot, 1)) S->projw.alloc(std::max<int64_t>(op->Mtot, 1));
+    launch_w_from_proj(op, nullptr, S->y.p, S->projw.p, s);  // proj = 0 (fhs_initialize_data_worker.m:43)
+    if (S->algo == FHS_ALGO_SARA) {
+      // sara.m:420-428: proj starts as the projection of G A x0 from zero.
+      // With v2 = 0 and gold = G A x0 the dual pass 1 gives d = G A x0 - y.
+      launch_degrid_dual_precond(op, 0, S->L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s, true);
+      launch_block_reduce_precond(op, 0, S->L, s);
+      launch_fb_iterations(op, 0, S->L, S->projw.p, S->y.p, S->fb_max, S->fb_min, S->fb_stop, s);
+    }
+  }
+  solver_update_weights(S);
+  FHS_CUDA(cudaStreamSynchronize(s));
+  solver_capture(S);
+  S->iter_done = 0;
+  S->ring_read = 0;
+  S->initialised = true;
+}
+
+}  // namespace fhs
+
+extern "C" {
+
 fhs_status fhs_solver_init(fhs_solver* s_, const double* xinit) {
-  return guarded_solver([&] {
-    Solver* S = sv(s_);
-    FHS_CHECK(S->params_set && S->data_set, FHS_ERR_STATE, "set data and params before init");
-    MeasOp* op = S->op;
-    DeviceGuard dg(op->device);
-    cudaStream_t s = op->stream;
-    if (!op->tuned) measop_autotune(op);   // before any state: the timed launches use scratch only
-    const int64_t n = (int64_t)S->L * S->N;
-    if (xinit) {
-      if (op->stage.n < (size_t)n) op->stage.alloc(n);
-      FHS_CUDA(cudaMemcpyAsync(op->stage.p, xinit, n * sizeof(double), cudaMemcpyHostToDevice, s));
-      launch_d2f(op->stage.p, S->x.p, n, s);
-    } else {
-      S->x.zero(s);
-    }
-    S->g.zero(s);
-    S->v1.zero(s);
-    S->v2.zero(s);
-    S->g1.zero(s);
-    if (S->nuclear) S->v0.zero(s);
-    S->ring_counter.zero(s);
-    // Fx_old: keep G A x_init per visibility (linearity of G)
-    if (!op->own_fft) launch_pad_real(op, S->x.p, 0, S->L, s);
-    solver_fft_forward(op, S->x.p, s);
-    launch_degrid_plain(op, 0, S->L, S->gold.p, s, true);
-    S->precond = op->precond;
-    if (S->precond) {
-      if (S->projw.n < (size_t)std::max<int64_t>(op->Mtot, 1)) S->projw.alloc(std::max<int64_t>(op->Mtot, 1));
-      launch_w_from_proj(op, nullptr, S->y.p, S->projw.p, s);  // proj = 0 (fhs_initialize_data_worker.m:43)
-      if (S->algo == FHS_ALGO_SARA) {
-        // sara.m:420-428: proj starts as the projection of G A x0 from zero.
-        // With v2 = 0 and gold = G A x0 the dual pass 1 gives d = G A x0 - y.
-        launch_degrid_dual_precond(op, 0, S->L, S->v2.p, S->gold.p, S->y.p, S->projw.p, s, true);
-        launch_block_reduce_precond(op, 0, S->L, s);
-        launch_fb_iterations(op, 0, S->L, S->projw.p, S->y.p, S->fb_max, S->fb_min, S->fb_stop, s);
-      }
-    }
-    solver_update_weights(S);
-    FHS_CUDA(cudaStreamSynchronize(s));
-    solver_capture(S);
-    S->iter_done = 0;
-    S->ring_read = 0;
-    S->initialised = true;
-  });
+  return guarded_solver([&] { solver_init_state(sv(s_), xinit, nullptr); });
 }
 
 // the iteration graph holds the operator's work lists and launch shapes:

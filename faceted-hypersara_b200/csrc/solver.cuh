@@ -59,4 +59,8 @@ struct Solver {
   ~Solver();
 };
 
+// fhs_solver_init from a host FP64 cube, a device FP32 cube [L][Nx][Ny]
+// (xinit_dev), or zeros (both NULL)
+void solver_init_state(Solver* S, const double* xinit, const float* xinit_dev);
+
 }  // namespace fhs

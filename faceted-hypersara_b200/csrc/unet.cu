@@ -825,6 +825,43 @@ void load_images(UNet* u, int N, int H, int W, const float* img, const float* tg
 
 }  // namespace
 
+namespace fhs {
+
+// input scale 1 / max|image| per image (1 for an all-zero image), one CTA
+// per image, as load_images does on the host
+__global__ void unet_image_scale_kernel(const float* __restrict__ img, int64_t np, float* __restrict__ scale) {
+  __shared__ float red[256];
+  const float* p = img + (size_t)blockIdx.x * np;
+  float m = 0.f;
+  for (int64_t i = threadIdx.x; i < np; i += blockDim.x) m = fmaxf(m, fabsf(p[i]));
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int k = 128; k > 0; k >>= 1) {
+    if (threadIdx.x < k) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + k]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) scale[blockIdx.x] = red[0] > 0.f ? 1.f / red[0] : 1.f;
+}
+
+void unet_forward_device(fhs_unet* h, int n, int H, int W, const float* d_img, float* d_out) {
+  UNet* u = checked_net(h);
+  FHS_CHECK(n >= 1 && d_img && d_out, FHS_ERR_INVALID_ARG, "bad arguments");
+  DeviceGuard g(u->device);
+  ensure_batch(u, n, H, W);
+  const int64_t np = (int64_t)H * W;
+  FHS_CUDA(cudaMemcpyAsync(u->img.p, d_img, (size_t)n * np * sizeof(float), cudaMemcpyDeviceToDevice, u->stream));
+  unet_image_scale_kernel<<<n, 256, 0, u->stream>>>(u->img.p, np, u->scale.p);
+  count_launch();
+  FHS_LAUNCH_CHECK();
+  forward(u);
+  FHS_CUDA(cudaMemcpyAsync(d_out, u->outp.p, (size_t)n * np * sizeof(float), cudaMemcpyDeviceToDevice, u->stream));
+  FHS_CUDA(cudaStreamSynchronize(u->stream));
+}
+
+int unet_device(const fhs_unet* h) { return checked_net(const_cast<fhs_unet*>(h))->device; }
+
+}  // namespace fhs
+
 extern "C" {
 
 fhs_status fhs_unet_create(int device, int base_channels, fhs_unet** out) {

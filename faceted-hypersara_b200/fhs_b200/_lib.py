@@ -73,6 +73,11 @@ class Tuning(C.Structure):
                             for i in range(self.n_grid)}}
 
 
+class WarmInfo(C.Structure):
+    _fields_ = [("used", C.c_int), ("objective_warm", C.c_double), ("objective_cold", C.c_double),
+                ("seconds", C.c_double)]
+
+
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
 _vp = C.c_void_p
@@ -139,6 +144,7 @@ SIGNATURES = {
     "fhs_unet_forward": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp]),
     "fhs_unet_gradient": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _dp]),
     "fhs_unet_train_step": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _fp, _fp, C.c_float, _dp]),
+    "fhs_solver_init_warm": (C.c_int, [_vp, _vp, C.c_int, C.POINTER(WarmInfo)]),
     "fhs_solver_group_stats": (C.c_int, [_vp, _dp]),
     "fhs_solver_update_weights": (C.c_int, [_vp]),
     "fhs_solver_ellipse_iterations": (C.c_int, [_vp, C.POINTER(C.c_int)]),

@@ -529,6 +529,15 @@ class Solver:
             xc = _cube_in(xinit, self.op.Ny, self.op.Nx)
             check(lib().fhs_solver_init(self._h, dptr(xc.reshape(-1, order="F"))))
 
+    def init_warm(self, net, chunk=16):
+        """Initialise from the learned warm start on the device (dirty cube,
+        network, fallback rule; fhs_solver_init_warm).  ``net``: a
+        ``warmstart.UNet`` on the solver's device.  Returns the decision record."""
+        info = LB.WarmInfo()
+        check(lib().fhs_solver_init_warm(self._h, net._h, int(chunk), C.byref(info)))
+        return {"used": bool(info.used), "objective_warm": info.objective_warm,
+                "objective_cold": info.objective_cold, "seconds": info.seconds}
+
     def iterate(self, n, record=True):
         info = (LB.IterInfo * max(n, 1))() if record else None
         check(lib().fhs_solver_iterate(self._h, n, info))

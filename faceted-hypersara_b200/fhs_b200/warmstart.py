@@ -165,18 +165,31 @@ def objective(x, op, y, eps, gamma, gamma0, n_groups, nlevel=4):
     """F(x) of the fallback rule (module docstring); x [Ny, Nx, L]."""
     from .api import HS_forward_operator_G, compute_sara_prior, nuclear_norm
     f = 0.0
+    if not np.any(x):   # Phi 0 = 0: only the data term, from y alone
+        for l in range(op.L):
+            for b, yb in enumerate(y[l]):
+                f += max(0.0, float(np.linalg.norm(np.asarray(yb))) - float(eps[l][b]))
+        return f
     Phix = HS_forward_operator_G(x, op)
     for l in range(op.L):
         for b, (pb, yb) in enumerate(zip(Phix[l], y[l])):
             f += max(0.0, float(np.linalg.norm(np.asarray(yb) - pb)) - float(eps[l][b]))
-    if not np.any(x):
-        return f
     lg = op.L // n_groups
+    g0 = np.ravel(gamma0)
+    Q = max(g0.size // n_groups, 1)   # gamma0 is group-major [g * Q + q]: the group's first facet weight
     for g in range(n_groups):
         xg = x[:, :, g * lg:(g + 1) * lg]
         f += float(np.ravel(gamma)[g]) * compute_sara_prior(xg, nlevel)
-        f += float(np.ravel(gamma0)[g]) * nuclear_norm(xg.reshape(-1, lg, order="F"))
+        f += float(g0[g * Q]) * nuclear_norm(xg.reshape(-1, lg, order="F"))
     return f
+
+
+def warm_start_device(net: UNet, solver, chunk=16):
+    """The same warm start and fallback rule with every cube kept on the
+    GPU (``fhs_solver_init_warm``): the solver (data and parameters set) is
+    initialised from the network's estimate or from zero; returns the
+    decision record."""
+    return solver.init_warm(net, chunk)
 
 
 def warm_start(net: UNet, op, y, eps, gamma, gamma0, n_groups=1, nlevel=4):

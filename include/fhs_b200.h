@@ -432,6 +432,25 @@ FHS_API fhs_status fhs_unet_gradient(fhs_unet* net, int n_images, int H, int W, 
 /* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss above */
 FHS_API fhs_status fhs_unet_train_step(fhs_unet* net, int n_images, int H, int W, const float* images,
                                        const float* targets, float lr, double* loss);
+/* fhs_solver_init from the learned warm start, on the device (no cube
+ * crosses to the host): the normalised dirty cube Re(Phi^H y) / PSF peak per
+ * channel (src/compute_residual_images.m:83-102 at x = 0) from the solver's
+ * operator and data, the network on every channel (chunk images per batch,
+ * <= 0: 16), clipped at 0, then the fallback rule: the solver starts from
+ * that estimate x0 if F(x0) < F(0), else from zero, with
+ *   F(x) = sum_b max(0, ||y_b - Phi_b x|| - eps_b)
+ *          + sum_g gamma_g ||Psi^T x_g||_{2,1} + sum_g gamma0_g ||x_g||_*
+ * (the nuclear term for the FHS / HS priors, over each whole spectral
+ * sub-cube with the group's first facet weight).  Needs set_data and
+ * set_params, a visibility (not DR) operator, image sides divisible by 8,
+ * and the network on the solver's device.  info may be NULL. */
+typedef struct fhs_warm_info {
+  int used;               /* 1: the solver starts from the network's estimate */
+  double objective_warm;  /* F(x0) */
+  double objective_cold;  /* F(0) */
+  double seconds;         /* host wall time of the call, initialisation included */
+} fhs_warm_info;
+FHS_API fhs_status fhs_solver_init_warm(fhs_solver* s, fhs_unet* net, int chunk, fhs_warm_info* info);
 
 /* Measurement hooks (no reference counterpart: the reference times its
  * phases with tic/toc, src/fhs/facetHyperSARA.m:703-716,771-776).

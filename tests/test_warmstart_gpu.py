@@ -94,3 +94,47 @@ def test_fallback_rejects_a_worse_start(trained):
     bad.close()
     op.close()
     assert not info["used"] and not np.any(x0)
+
+
+def test_device_warm_start_matches_the_host_route(trained):
+    """fhs_solver_init_warm (every cube on the GPU) takes the same decision
+    as the host route and starts from the same estimate: the dirty cubes
+    differ at FP32 rounding level (hand-written vs library FFT), which the
+    BF16 network passes on at the 2e-2 level of the network tests."""
+    from fhs_b200 import warmstart as ws
+    from fhs_b200._lib import ALGO_HS
+    from fhs_b200.api import Solver
+    from helpers import rel
+    net, _ = trained
+    x, op, y, eps, param = _problem(557)
+    x0_h, info_h = ws.warm_start(net, op, y, eps, param["gamma"], param["gamma0"])
+    s = Solver(op, ALGO_HS, param)
+    s.set_data(y, eps)
+    dec = ws.warm_start_device(net, s)
+    assert dec["used"] == info_h["used"] and dec["used"]
+    assert rel(s.x(), x0_h) < 2e-2
+    assert abs(dec["objective_cold"] - info_h["objective_cold"]) < 1e-4 * info_h["objective_cold"]
+    assert abs(dec["objective_warm"] - info_h["objective_warm"]) < 1e-2 * info_h["objective_warm"]
+    s.iterate(5)   # the solver runs from the warm start
+    assert _snr(np.moveaxis(x, 0, 2), s.x()) > _snr(np.moveaxis(x, 0, 2), x0_h)
+    s.close()
+    op.close()
+
+
+def test_device_fallback_starts_from_zero(trained):
+    from fhs_b200 import warmstart as ws
+    from fhs_b200._lib import ALGO_HS
+    from fhs_b200.api import Solver
+    net, _ = trained
+    q = net.params().copy()
+    q[-33:-1] *= 1e3   # the 1x1 head weights
+    bad = ws.UNet(params=q)
+    x, op, y, eps, param = _problem(558)
+    s = Solver(op, ALGO_HS, param)
+    s.set_data(y, eps)
+    dec = ws.warm_start_device(bad, s)
+    bad.close()
+    assert not dec["used"] and dec["objective_warm"] > dec["objective_cold"]
+    assert not np.any(s.x())
+    s.close()
+    op.close()
