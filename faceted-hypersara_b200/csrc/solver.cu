@@ -853,14 +853,24 @@ fhs_status fhs_solver_run(fhs_solver* s_, int max_iter, fhs_run_info* out) {
     bool adjust = S->adjust_noise;
     if (adjust) upload_betas(S, true);  // priors off until the first adjustment
     ensure_graph(S);
+    // The stopping statistics stay in the device ring until a test needs
+    // them: while t - last < pdfb_min_iter (and no noise adjustment is
+    // pending) the PDFB test cannot fire, so the graphs are launched back to
+    // back and their records read together at the next test.
+    int pending = 0;
     for (t = 1; t <= max_iter; ++t) {
       FHS_CUDA(cudaGraphLaunch(S->graph, s));
       g_launches += S->launches_per_iter;
-      read_ring(S, S->iter_done, 1, rec);
       S->iter_done += 1;
-      fill_info(S, rec.data(), &info);
-      FHS_CHECK(std::isfinite(info.rel_val) && std::isfinite(info.residual), FHS_ERR_NUMERIC,
-                "non-finite iterate at iteration " + std::to_string(t));
+      ++pending;
+      if (!adjust && t - last < S->pdfb_min && t < max_iter && pending < kReportRing / 2) continue;
+      read_ring(S, S->iter_done - pending, pending, rec);
+      for (int i = 0; i < pending; ++i) {
+        fill_info(S, rec.data() + (size_t)i * S->G * kReportFields, &info);
+        FHS_CHECK(std::isfinite(info.rel_val) && std::isfinite(info.residual), FHS_ERR_NUMERIC,
+                  "non-finite iterate at iteration " + std::to_string(t - pending + 1 + i));
+      }
+      pending = 0;
       const bool pdfb = (t - last >= S->pdfb_min) &&
                         (t - last >= S->pdfb_max ||
                          (info.rel_val <= S->pdfb_rel_var && info.residual <= S->pdfb_tol * info.epsilon) ||
