@@ -145,6 +145,8 @@ struct LevelArgs {
   int64_t in_stride, s_stride, apx_stride;
   int first, last;   // input from x (level 1); A into coef (level J)
   float in_scale;
+  int dirac;          // level 1 of the split kernel: the db1 tiles also prox the Dirac rows
+  int64_t dirac_off;  // first Dirac row in a channel's coefficient vector
 };
 
 __global__ void __launch_bounds__(256) analysis_kernel(LevelArgs a, const float* __restrict__ x,
@@ -515,7 +517,8 @@ __device__ __forceinline__ void ap_split_xfilter(const LevelArgs& a, int b, int 
 // steps 2-3 of the split kernel for branch BR: the dual of the branch's two
 // subbands, the y filtering accumulated into it, the weighted l21 prox
 template <int MAXL, int LF, bool LAST, int BR>
-__device__ __forceinline__ void ap_split_tail(const LevelArgs& a, int b, int tile, int g, float* __restrict__ apx,
+__device__ __forceinline__ void ap_split_tail(const LevelArgs& a, int b, int tile, int g, const float* __restrict__ x,
+                                              float* __restrict__ apx,
                                               float* __restrict__ v1, const float* __restrict__ weights,
                                               const double* __restrict__ beta, int lg,
                                               double* __restrict__ l21_acc, const float* sm, double* red) {
@@ -594,6 +597,39 @@ __device__ __forceinline__ void ap_split_tail(const LevelArgs& a, int b, int til
     prox(w0, off0);
     if (PROX1) prox(w1, off1);
   }
+  if constexpr (LF == 2) {
+    // level 1, db1: a tile's input block (64 rows x 16 columns, no halo) is
+    // a partition of the image, so these CTAs also take the Dirac rows of
+    // their pixels (coefficients xhat / 3), two pixels per thread
+    if (a.dirac) {
+      const float bt = (float)beta[g];
+      const int n0i = a.n0[0], n1i = a.n1[0];
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        const int k = threadIdx.x + h * kApSplitThreads;
+        const int r = 2 * AT0 * tp0 + (k & (2 * AT0 - 1)), c = 2 * AT1 * tp1 + k / (2 * AT0);
+        if (r >= n0i || c >= n1i) continue;
+        const int64_t pix = (int64_t)c * n0i + r, i = a.dirac_off + pix;
+        float w[MAXL];
+        float ss = 0.f;
+#pragma unroll
+        for (int l = 0; l < MAXL; ++l) {
+          w[l] = 0.f;
+          if (l < nch) {
+            const size_t plane = (size_t)g * lg + l;
+            w[l] = v1[plane * a.s_stride + i] + __ldg(x + plane * a.in_stride + pix) * (1.f / 3.f);
+            ss = fmaf(w[l], w[l], ss);
+          }
+        }
+        const float l2 = sqrtf(ss);
+        l21 += l2;
+        const float soft = fmaxf(l2 - bt * weights[(size_t)g * a.s_stride + i], 0.f) / (l2 + 2.220446049250313e-16f);
+#pragma unroll
+        for (int l = 0; l < MAXL; ++l)
+          if (l < nch) v1[((size_t)g * lg + l) * a.s_stride + i] = w[l] - soft * w[l];
+      }
+    }
+  }
   if (l21_acc) {
     for (int sh = 16; sh > 0; sh >>= 1) l21 += __shfl_down_sync(0xffffffffu, l21, sh);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l21;
@@ -622,14 +658,14 @@ __global__ void __launch_bounds__(kApSplitThreads, 2) analysis_prox_split_kernel
     ap_split_xfilter<LFV>(a, b, tile, g, x, apx, lg, sm_ap);                                            \
     if (a.last) {                                                                                       \
       if (br == 0)                                                                                      \
-        ap_split_tail<MAXL, LFV, true, 0>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red);  \
+        ap_split_tail<MAXL, LFV, true, 0>(a, b, tile, g, x, apx, v1, weights, beta, lg, l21_acc, sm_ap, red);  \
       else                                                                                              \
-        ap_split_tail<MAXL, LFV, true, 1>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red);  \
+        ap_split_tail<MAXL, LFV, true, 1>(a, b, tile, g, x, apx, v1, weights, beta, lg, l21_acc, sm_ap, red);  \
     } else {                                                                                            \
       if (br == 0)                                                                                      \
-        ap_split_tail<MAXL, LFV, false, 0>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); \
+        ap_split_tail<MAXL, LFV, false, 0>(a, b, tile, g, x, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); \
       else                                                                                              \
-        ap_split_tail<MAXL, LFV, false, 1>(a, b, tile, g, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); \
+        ap_split_tail<MAXL, LFV, false, 1>(a, b, tile, g, x, apx, v1, weights, beta, lg, l21_acc, sm_ap, red); \
     }                                                                                                   \
     break;
   switch (b) { FHS_C(0, 2) FHS_C(1, 4) FHS_C(2, 6) FHS_C(3, 8) FHS_C(4, 10) FHS_C(5, 12) FHS_C(6, 14) FHS_C(7, 16) }
@@ -1031,6 +1067,8 @@ void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* 
     a.first = j == 1;
     a.last = j == p.J;
     a.in_scale = j == 1 ? 1.f / 3.f : 1.f;
+    a.dirac = (j == 1 && lg <= kApChunk) ? 1 : 0;   // the split kernel's db1 tiles take the Dirac rows
+    a.dirac_off = p.boff[kSaraWavelets];
     dim3 grid(ceil_div(maxt, kApBand) * kSaraWavelets * kApBand, n_groups);
 #define FHS_AP(MAXL) launch_analysis_prox<MAXL>(grid, s, a, xhat, apx, v1, weights, beta, lg, l21_acc)
     if (lg <= 1)
@@ -1047,6 +1085,7 @@ void sara_analysis_prox(const SaraPlan& p, const float* xhat, float* v1, float* 
     count_launch();
     FHS_LAUNCH_CHECK();
   }
+  if (lg <= kApChunk) return;   // the Dirac rows went with level 1's db1 tiles
   // Dirac part: coefficients are xhat/3
   const int64_t npix = (int64_t)p.Ny * p.Nx;
   const int64_t off = p.boff[kSaraWavelets];
