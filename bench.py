@@ -197,7 +197,7 @@ def algorithmic_bytes(prob, sp_s, fb_counts=None):
 _MB = 1e6
 TRAFFIC_PER_LAUNCH = {
     "grid_dual": 4 * (450 + 335) * _MB,
-    "sara_analysis_prox": 4 * (872 + 599 + 138 + 23) * _MB,
+    "sara_analysis_prox": 4 * (947 + 667) * _MB,
     "sara_synthesis": 4 * (819 + 156) * _MB,
     "degrid_dual": 4 * (691 + 157) * _MB,
     "fft_inverse": 4 * (537 + 118 + 134 + 35) * _MB,
